@@ -1,0 +1,102 @@
+/*
+ * sinvb.h -- C ABI of libsinvb.so, the B200 (sm_100a) selected-inversion library.
+ *
+ * Selected inversion of a block-tridiagonal matrix A with n diagonal blocks
+ * of size b x b: the diagonal blocks G_ii, the upper blocks G_{i,i+1} and the
+ * lower blocks G_{i+1,i} of G = A^{-1}.
+ *
+ * Block-array layout (the reference's ``convertDenseToBlkTridiag``,
+ * src/sinv/utils/matrices_utils.py:115-151): ``diag`` holds n blocks,
+ * ``upper`` n-1 blocks A_{i,i+1}, ``lower`` n-1 blocks A_{i+1,i}; every
+ * block is b x b, row-major, contiguous, blocks back to back.  Complex
+ * element types are interleaved (re, im) pairs (C99 / numpy / torch layout).
+ *
+ * All pointers are device pointers.  Every call is asynchronous on
+ * ``stream``: it validates arguments on the host (negative return codes),
+ * enqueues its kernels and returns.  Conditions found on the device (a zero
+ * or non-finite pivot in the pivot-free elimination, a wait that gave up)
+ * are written to a status word inside the caller's workspace and read back
+ * with ``sinvb_workspace_status``.  The library never allocates or frees
+ * device memory of its own in these entry points: the caller passes a
+ * workspace of at least ``sinvb_*_workspace_size`` bytes.  Inputs are never
+ * modified.  Calls on different streams with different workspaces may run
+ * concurrently.
+ */
+#ifndef SINVB_H
+#define SINVB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* sinvb_stream_t; /* == cudaStream_t */
+
+/* ---- return / status codes ------------------------------------------- */
+#define SINVB_OK 0
+#define SINVB_EINVAL (-1)      /* bad argument (null pointer, size, flags)     */
+#define SINVB_ECUDA (-2)       /* a CUDA runtime call failed                   */
+#define SINVB_EWORKSPACE (-3)  /* workspace too small or misaligned            */
+#define SINVB_EUNSUPPORTED (-4)/* no B200 / sm_100 device, or feature missing  */
+/* device-detected, reported through the workspace status word (>0) */
+#define SINVB_STATUS_PIVOT 1   /* zero or non-finite pivot in a block inverse  */
+#define SINVB_STATUS_TIMEOUT 2 /* a bounded device wait gave up                */
+
+/* ---- flags -------------------------------------------------------------- */
+/* rgf.py:19 sym_mat: G_{i,i+1} = G_{i+1,i}^T (plain transpose, rgf.py:57-58) */
+#define SINVB_SYM 1u
+/* rgf.py:20 save_off_diag: write G_upper / G_lower (rgf.py:55) */
+#define SINVB_SAVE_OFFDIAG 2u
+/* run the sweep with the whole GPU as one team (cooperative launch) even for
+ * small blocks; by default the library picks the team from b */
+#define SINVB_FORCE_GRID 4u
+#define SINVB_FORCE_CTA 8u
+
+/* ---- element type codes --------------------------------------------------- */
+#define SINVB_C128 0 /* complex double */
+#define SINVB_F64 1  /* double         */
+#define SINVB_C64 2  /* complex float  (computed in FP64, rounded on output) */
+#define SINVB_F32 3  /* float          (computed in FP64, rounded on output) */
+
+/* Library / device info. */
+int sinvb_version(void);
+const char* sinvb_status_string(int code);
+
+/* Bytes of workspace one ``sinvb_rgf_*`` call needs (256-byte aligned). */
+size_t sinvb_rgf_workspace_size(int n, int b, int dtype, unsigned flags);
+
+/*
+ * Serial RGF selected inversion.
+ * Replaces ``rgf(A, sym_mat, save_off_diag)`` of
+ * src/sinv/algorithms/rgf/rgf.py:17-64 (forward sweep :44-48, backward sweep
+ * :51-62) in the block-array form of
+ * src/sinv/algorithms/rgf/rgf2sided.py:18-24.
+ * G_upper / G_lower may be NULL when SINVB_SAVE_OFFDIAG is not set.
+ */
+int sinvb_rgf_z(const void* diag, const void* upper, const void* lower, int n, int b,
+                unsigned flags, void* G_diag, void* G_upper, void* G_lower,
+                void* workspace, size_t workspace_bytes, sinvb_stream_t stream);
+int sinvb_rgf_d(const void* diag, const void* upper, const void* lower, int n, int b,
+                unsigned flags, void* G_diag, void* G_upper, void* G_lower,
+                void* workspace, size_t workspace_bytes, sinvb_stream_t stream);
+int sinvb_rgf_c(const void* diag, const void* upper, const void* lower, int n, int b,
+                unsigned flags, void* G_diag, void* G_upper, void* G_lower,
+                void* workspace, size_t workspace_bytes, sinvb_stream_t stream);
+int sinvb_rgf_s(const void* diag, const void* upper, const void* lower, int n, int b,
+                unsigned flags, void* G_diag, void* G_upper, void* G_lower,
+                void* workspace, size_t workspace_bytes, sinvb_stream_t stream);
+
+/*
+ * Device status word of a workspace: synchronises ``stream`` and returns the
+ * status (SINVB_OK or a positive SINVB_STATUS_*) in *status.  The word is
+ * reset by the next call that uses the workspace.
+ */
+int sinvb_workspace_status(const void* workspace, sinvb_stream_t stream, int* status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SINVB_H */

@@ -1,0 +1,6 @@
+"""Selected-inversion algorithms, mirroring ``sinv.algorithms``
+(``src/sinv/algorithms/__init__.py:3-9``): ``rgf`` is the RGF module
+(``rgf.rgf(...)``).  The MPI-distributed algorithms of the reference
+(rgf2sided, bcr_parallel, psr, pdiv) are not part of this library."""
+
+from . import rgf  # noqa: F401

@@ -1,0 +1,198 @@
+// Pivot-free in-place block inversion (Gauss-Jordan).
+//
+// The reference inverts every block with numpy.linalg.inv (LAPACK getrf/getri
+// with partial pivoting, src/sinv/algorithms/rgf/rgf.py:44,48).  The RGF and
+// BCR recursions have no pivoting across blocks; inside a block this library
+// eliminates without pivoting as well and reports a zero or non-finite pivot
+// through the workspace status word (SINVB_STATUS_PIVOT) instead of trapping.
+//
+// Gauss-Jordan on an m x m matrix, step k (p = a_kk):
+//   a_kk <- 1/p,  a_kj <- a_kj/p,  a_ik <- -a_ik/p,  a_ij <- a_ij - a_ik a_kj/p
+// After m steps the array holds the inverse; m^3 multiply-adds in total.
+//
+// * cta_gj_invert: one CTA, m <= 64.  The block lives in registers (thread
+//   (ty, tx) of a 16 x 16 grid owns rows ty+16r and columns tx+16c); row k,
+//   column k and 1/a_kk are published through double-buffered shared arrays,
+//   so one barrier per step suffices.
+// * team_invert: any m.  Blocked Gauss-Jordan over 64-wide panels:
+//   (1) invert the diagonal panel block with cta_gj_invert,
+//   (2) scale the row panel by it (DMMA GEMM, in place),
+//   (3) rank-64 update of every other block and the new column panel
+//       (DMMA GEMMs), the column panel going to a side buffer that is copied
+//       back while the next pivot block is inverted.
+#pragma once
+
+#include "block_gemm.cuh"
+
+namespace sinvb {
+
+constexpr int kPanel = 64;
+
+template <class T>
+struct GjShared {
+  T rowbuf[2][kPanel];
+  T colbuf[2][kPanel];
+  T pinv[2];
+};
+
+// Inverts the m x m block at a (leading dimension lda), m <= 64, in place.
+// Returns false (and reports) on a zero / non-finite pivot; the block then
+// holds non-finite values.
+template <class T>
+__device__ bool cta_gj_invert(T* a, int lda, int m, WsHeader* hdr, int detail, void* smem_raw) {
+  GjShared<T>& sh = *reinterpret_cast<GjShared<T>*>(smem_raw);
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  T v[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; r++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      int i = ty + 16 * r, j = tx + 16 * c;
+      v[r][c] = (i < m && j < m) ? a[(size_t)i * lda + j] : Elem<T>::zero();
+    }
+  __syncthreads();  // smem may still be read by a previous user
+  // publish column 0, row 0 and 1/a_00
+#pragma unroll
+  for (int r = 0; r < 4; r++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      int i = ty + 16 * r, j = tx + 16 * c;
+      if (j == 0 && i < m) sh.colbuf[0][i] = v[r][c];
+      if (i == 0 && j < m) sh.rowbuf[0][j] = v[r][c];
+      if (i == 0 && j == 0) sh.pinv[0] = recip(v[r][c]);
+    }
+  bool bad = false;
+  for (int k = 0; k < m; k++) {
+    __syncthreads();
+    const int buf = k & 1, nbuf = buf ^ 1;
+    const T ip = sh.pinv[buf];
+    if (tid == 0 && !bad && !pivot_ok(sh.rowbuf[buf][k])) {
+      bad = true;
+      report(hdr, SINVB_STATUS_PIVOT, detail);
+    }
+    T rk[4], ck[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      int j = tx + 16 * c;
+      rk[c] = j < m ? sh.rowbuf[buf][j] * ip : Elem<T>::zero();
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      int i = ty + 16 * r;
+      ck[r] = i < m ? sh.colbuf[buf][i] : Elem<T>::zero();
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        int i = ty + 16 * r, j = tx + 16 * c;
+        T x = v[r][c];
+        if (i == k) {
+          x = (j == k) ? ip : rk[c];
+        } else if (j == k) {
+          x = -(ck[r] * ip);
+        } else {
+          x = fms(x, ck[r], rk[c]);
+        }
+        v[r][c] = x;
+        if (k + 1 < m) {
+          if (j == k + 1 && i < m) sh.colbuf[nbuf][i] = x;
+          if (i == k + 1 && j < m) sh.rowbuf[nbuf][j] = x;
+          if (i == k + 1 && j == k + 1) sh.pinv[nbuf] = recip(x);
+        }
+      }
+  }
+#pragma unroll
+  for (int r = 0; r < 4; r++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      int i = ty + 16 * r, j = tx + 16 * c;
+      if (i < m && j < m) a[(size_t)i * lda + j] = v[r][c];
+    }
+  __syncthreads();
+  return !bad;
+}
+
+// Copies a rows x cols rectangle (optionally transposed: dst[j][i] = src[i][j]),
+// split over the team's CTAs.  No synchronisation.
+template <class T, class Team>
+__device__ void team_copy(Team& team, int rows, int cols, const T* src, int lds, T* dst, int ldd,
+                          bool transpose = false) {
+  const size_t total = (size_t)rows * cols;
+  const size_t stride = (size_t)team.size() * blockDim.x;
+  for (size_t e = (size_t)team.rank() * blockDim.x + threadIdx.x; e < total; e += stride) {
+    int i = (int)(e / cols), j = (int)(e % cols);
+    if (transpose)
+      dst[(size_t)j * ldd + i] = src[(size_t)i * lds + j];
+    else
+      dst[(size_t)i * ldd + j] = src[(size_t)i * lds + j];
+  }
+}
+
+// Bytes of side buffer team_invert needs for an m x m block.
+__host__ __device__ inline size_t invert_side_elems(int m) { return m > kPanel ? (size_t)m * kPanel : 0; }
+
+// Inverts the m x m block at a (lda) in place with the whole team.  W is a side
+// buffer of invert_side_elems(m) elements.  Starts and ends with the block
+// visible to the whole team (the caller synchronised before; this function
+// synchronises after).  Returns false when a team barrier gave up.
+template <class T, int BM, int BN, class Team>
+__device__ bool team_invert(Team& team, T* a, int lda, int m, T* W, WsHeader* hdr, int detail, T* smem) {
+  if (m <= kPanel) {
+    if (team.rank() == 0) cta_gj_invert<T>(a, lda, m, hdr, detail, smem);
+    return team.sync();
+  }
+  const int np = (m + kPanel - 1) / kPanel;
+  int prevK0 = -1, prevkb = 0;
+  for (int p = 0; p < np; p++) {
+    const int K0 = p * kPanel, kb = min(kPanel, m - K0);
+    T* Dinv = a + (size_t)K0 * lda + K0;
+    // (1) invert the pivot block; copy back the previous column panel
+    if (team.rank() == 0) cta_gj_invert<T>(Dinv, lda, kb, hdr, detail, smem);
+    if (prevK0 >= 0) {
+      // rows above and below the previous panel
+      team_copy<T>(team, prevK0, prevkb, W, kPanel, a + prevK0, lda);
+      int r1 = prevK0 + prevkb;
+      team_copy<T>(team, m - r1, prevkb, W + (size_t)r1 * kPanel, kPanel, a + (size_t)r1 * lda + prevK0, lda);
+    }
+    if (!team.sync()) return false;
+    // (2) row panel: A[K, J] <- Dinv * A[K, J], J left / right of the panel
+    {
+      GemmOp<T> ops[2];
+      int right = K0 + kb;
+      ops[0] = make_op<T>(kb, K0, kb, 1.0, Dinv, lda, a + (size_t)K0 * lda, lda, nullptr, 0,
+                          a + (size_t)K0 * lda, lda);
+      ops[1] = make_op<T>(kb, m - right, kb, 1.0, Dinv, lda, a + (size_t)K0 * lda + right, lda, nullptr, 0,
+                          a + (size_t)K0 * lda + right, lda);
+      team_gemm<T, BM, BN>(team, ops, 2, smem);
+    }
+    if (!team.sync()) return false;
+    // (3) A[I, J] -= A[I, K] A[K, J] for I, J outside the panel; W[I] = -A[I, K] Dinv
+    {
+      GemmOp<T> ops[6];
+      int right = K0 + kb;
+      int rs[2] = {0, right}, rn[2] = {K0, m - right};
+      int q = 0;
+      for (int ri = 0; ri < 2; ri++) {
+        const T* colK = a + (size_t)rs[ri] * lda + K0;
+        for (int ci = 0; ci < 2; ci++) {
+          const T* rowK = a + (size_t)K0 * lda + rs[ci];
+          T* C = a + (size_t)rs[ri] * lda + rs[ci];
+          ops[q++] = make_op<T>(rn[ri], rn[ci], kb, -1.0, colK, lda, rowK, lda, C, lda, C, lda);
+        }
+        ops[q++] = make_op<T>(rn[ri], kb, kb, -1.0, colK, lda, Dinv, lda, nullptr, 0,
+                              W + (size_t)rs[ri] * kPanel, kPanel);
+      }
+      team_gemm<T, BM, BN>(team, ops, q, smem);
+    }
+    if (!team.sync()) return false;
+    prevK0 = K0;
+    prevkb = kb;
+  }
+  team_copy<T>(team, prevK0, prevkb, W, kPanel, a + prevK0, lda);
+  int r1 = prevK0 + prevkb;
+  team_copy<T>(team, m - r1, prevkb, W + (size_t)r1 * kPanel, kPanel, a + (size_t)r1 * lda + prevK0, lda);
+  return team.sync();
+}
+
+}  // namespace sinvb

@@ -1,0 +1,115 @@
+// The RGF selected-inversion sweep on one team of CTAs.
+//
+// Reference: src/sinv/algorithms/rgf/rgf.py:17-64.
+//   forward  (rgf.py:44-48):  g_0 = A_00^{-1},
+//                             g_i = (A_ii - A_{i,i-1} g_{i-1} A_{i-1,i})^{-1}
+//   backward (rgf.py:51-62):  lf = G_{i+1} A_{i+1,i} g_i
+//                             G_{i+1,i} = -lf
+//                             G_{i,i+1} = -g_i A_{i,i+1} G_{i+1}   (or G_{i+1,i}^T if sym)
+//                             G_ii      = g_i + g_i A_{i,i+1} lf
+//
+// Schedule (6 block products per block row instead of the reference's 8):
+//   forward step i:  X_{i-1} = g_{i-1} U_{i-1},  P_i = L_i g_{i-1}     (phase F1)
+//                    S_i = A_ii - P_i U_{i-1}                          (phase F2)
+//                    g_i = S_i^{-1} in place                           (team_invert)
+//   backward step i: T   = -G_{i+1} P_{i+1}           (= G_{i+1,i})    (phase B1)
+//                    G_{i,i+1} = -X_i G_{i+1}                          (phase B2)
+//                    G_ii = g_i - X_i T                                (phase B2)
+// with U_i = A_{i,i+1}, L_{i+1} = A_{i+1,i}.  (A g) A and G (A g) replace the
+// reference's (G A) g association; the difference is rounding only.
+//
+// Storage: g_i is built in G_diag[i].  With SAVE_OFFDIAG, X_i lives in
+// G_lower[i] and P_{i+1} in G_upper[i] until the backward step overwrites
+// them; otherwise both live in the workspace.  T alternates between two
+// workspace blocks and is copied to G_lower[i] one phase later.
+#pragma once
+
+#include "block_inverse.cuh"
+
+namespace sinvb {
+
+template <class T>
+struct RgfParams {
+  const T* diag;
+  const T* upper;
+  const T* lower;
+  T* Gd;
+  T* Gu;
+  T* Gl;
+  T* X;    // n-1 blocks (may alias Gl)
+  T* P;    // n-1 blocks (may alias Gu)
+  T* T0;   // b*b
+  T* T1;   // b*b
+  T* Winv; // invert_side_elems(b)
+  WsHeader* hdr;
+  int n, b;
+  unsigned flags;
+};
+
+template <class T, int BM, int BN, class Team>
+__device__ void rgf_sweep(Team& team, const RgfParams<T>& p, T* smem) {
+  const int n = p.n, b = p.b;
+  const size_t bb = (size_t)b * b;
+  const bool sym = p.flags & SINVB_SYM;
+  const bool save = p.flags & SINVB_SAVE_OFFDIAG;
+
+  // g_0 = A_00^{-1}
+  team_copy<T>(team, b, b, p.diag, b, p.Gd, b);
+  if (!team.sync()) return;
+  if (!team_invert<T, BM, BN>(team, p.Gd, b, b, p.Winv, p.hdr, 0, smem)) return;
+
+  for (int i = 1; i < n; i++) {
+    const T* g = p.Gd + (i - 1) * bb;
+    const T* U = p.upper + (i - 1) * bb;
+    const T* L = p.lower + (i - 1) * bb;
+    {  // F1
+      GemmOp<T> ops[2];
+      ops[0] = make_op<T>(b, b, b, 1.0, g, b, U, b, nullptr, 0, p.X + (i - 1) * bb, b);
+      ops[1] = make_op<T>(b, b, b, 1.0, L, b, g, b, nullptr, 0, p.P + (i - 1) * bb, b);
+      team_gemm<T, BM, BN>(team, ops, 2, smem);
+    }
+    if (!team.sync()) return;
+    {  // F2: S_i = A_ii - P_i U_{i-1}
+      GemmOp<T> op = make_op<T>(b, b, b, -1.0, p.P + (i - 1) * bb, b, U, b, p.diag + i * bb, b,
+                                p.Gd + i * bb, b);
+      team_gemm<T, BM, BN>(team, &op, 1, smem);
+    }
+    if (!team.sync()) return;
+    if (!team_invert<T, BM, BN>(team, p.Gd + i * bb, b, b, p.Winv, p.hdr, i, smem)) return;
+  }
+
+  T* prevT = nullptr;
+  int prevI = -1;
+  for (int i = n - 2; i >= 0; i--) {
+    T* Tcur = (i & 1) ? p.T1 : p.T0;
+    {  // B1: T = -G_{i+1} P_{i+1}; flush the previous T into G_lower / G_upper
+      GemmOp<T> op = make_op<T>(b, b, b, -1.0, p.Gd + (i + 1) * bb, b, p.P + i * bb, b, nullptr, 0, Tcur, b);
+      team_gemm<T, BM, BN>(team, &op, 1, smem);
+      if (prevT && save) {
+        team_copy<T>(team, b, b, prevT, b, p.Gl + prevI * bb, b);
+        if (sym) team_copy<T>(team, b, b, prevT, b, p.Gu + prevI * bb, b, true);
+      }
+    }
+    if (!team.sync()) return;
+    {  // B2
+      GemmOp<T> ops[2];
+      int q = 0;
+      const T* X = p.X + i * bb;
+      if (save && !sym)
+        ops[q++] = make_op<T>(b, b, b, -1.0, X, b, p.Gd + (i + 1) * bb, b, nullptr, 0, p.Gu + i * bb, b);
+      T* Gii = p.Gd + i * bb;
+      ops[q++] = make_op<T>(b, b, b, -1.0, X, b, Tcur, b, Gii, b, Gii, b);
+      team_gemm<T, BM, BN>(team, ops, q, smem);
+    }
+    if (!team.sync()) return;
+    prevT = Tcur;
+    prevI = i;
+  }
+  if (prevT && save) {
+    team_copy<T>(team, b, b, prevT, b, p.Gl + prevI * bb, b);
+    if (sym) team_copy<T>(team, b, b, prevT, b, p.Gu + prevI * bb, b, true);
+    team.sync();
+  }
+}
+
+}  // namespace sinvb
