@@ -95,6 +95,49 @@ int sinvb_rgf_s(const void* diag, const void* upper, const void* lower, int n, i
  */
 int sinvb_workspace_status(const void* workspace, sinvb_stream_t stream, int* status);
 
+/* ---- batched RGF: many independent matrices in one persistent launch ------- */
+/*
+ * One matrix of a batch (block arrays as above; every instance may have its
+ * own n and b).  This is the energy loop of a transport calculation: the
+ * reference calls rgf (src/sinv/algorithms/rgf/rgf.py:17) once per matrix
+ * A(E_k) = E_k I - H - Sigma(E_k); here one launch walks every instance's
+ * sweep, instances dispatched largest-first from a device work queue, one
+ * team of CTAs per instance.
+ */
+typedef struct sinvb_batch_desc {
+  const void* diag;
+  const void* upper;
+  const void* lower;
+  void* G_diag;
+  void* G_upper;
+  void* G_lower;
+  int n;
+  int b;
+} sinvb_batch_desc;
+
+/* precision modes of the batched call (the ``flags`` argument, high bits) */
+#define SINVB_PREC_FP64 0u          /* every product in FP64 (DMMA)             */
+#define SINVB_PREC_MIXED (1u << 8)  /* block products on tcgen05, FP64 inverses */
+
+size_t sinvb_rgf_batched_workspace_size(const sinvb_batch_desc* descs, int count, int dtype, unsigned flags);
+
+/*
+ * Uploads the descriptors into the workspace (ordered by cost) and launches
+ * the persistent kernel.  ``status`` (optional, device, ``count`` ints) gets
+ * each instance's device status, indexed like ``descs``.
+ */
+int sinvb_rgf_batched_z(const sinvb_batch_desc* descs, int count, unsigned flags, void* workspace,
+                        size_t workspace_bytes, int* status, sinvb_stream_t stream);
+int sinvb_rgf_batched_d(const sinvb_batch_desc* descs, int count, unsigned flags, void* workspace,
+                        size_t workspace_bytes, int* status, sinvb_stream_t stream);
+/*
+ * Re-runs the batch last uploaded into ``workspace`` (same descriptors, same
+ * buffers) with no host-to-device traffic: one memset and one kernel launch,
+ * suitable for stream capture into a CUDA graph.
+ */
+int sinvb_rgf_batched_rerun_z(void* workspace, sinvb_stream_t stream);
+int sinvb_rgf_batched_rerun_d(void* workspace, sinvb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

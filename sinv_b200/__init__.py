@@ -8,5 +8,6 @@ replaces ``sinv.algorithms.rgf.rgf`` and ``sinv_b200.utils.matu`` replaces
 
 from . import algorithms, utils  # noqa: F401
 from .algorithms.rgf import rgf, rgf_blocks  # noqa: F401
+from .algorithms.batched import BatchPlan, rgf_batched  # noqa: F401
 
-__all__ = ["algorithms", "utils", "rgf", "rgf_blocks"]
+__all__ = ["algorithms", "utils", "rgf", "rgf_blocks", "rgf_batched", "BatchPlan"]

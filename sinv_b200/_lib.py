@@ -44,7 +44,21 @@ SIGNATURES = {
     "sinvb_rgf_c": (_i, _RGF_ARGS),
     "sinvb_rgf_s": (_i, _RGF_ARGS),
     "sinvb_workspace_status": (_i, [_vp, _vp, ctypes.POINTER(_i)]),
+    "sinvb_rgf_batched_workspace_size": (_sz, [_vp, _i, _i, _u]),
+    "sinvb_rgf_batched_z": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp]),
+    "sinvb_rgf_batched_d": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp]),
+    "sinvb_rgf_batched_rerun_z": (_i, [_vp, _vp]),
+    "sinvb_rgf_batched_rerun_d": (_i, [_vp, _vp]),
 }
+
+PREC_FP64 = 0
+PREC_MIXED = 1 << 8
+
+
+class BatchDesc(ctypes.Structure):
+    """``sinvb_batch_desc`` of include/sinvb.h."""
+    _fields_ = [("diag", _vp), ("upper", _vp), ("lower", _vp), ("G_diag", _vp), ("G_upper", _vp),
+                ("G_lower", _vp), ("n", _i), ("b", _i)]
 
 
 class SinvbUnavailable(RuntimeError):

@@ -4,3 +4,5 @@
 (rgf2sided, bcr_parallel, psr, pdiv) are not part of this library."""
 
 from . import rgf  # noqa: F401
+from . import batched  # noqa: F401
+from .batched import BatchPlan, rgf_batched  # noqa: F401

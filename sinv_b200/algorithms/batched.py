@@ -1,0 +1,142 @@
+"""Batched RGF: many independent selected inversions in one persistent launch.
+
+The reference solves one matrix per ``rgf`` call
+(``src/sinv/algorithms/rgf/rgf.py:17``); a transport code calls it once per
+energy point A(E_k) = E_k I - H - Sigma(E_k).  ``rgf_batched`` takes the whole
+list (each instance with its own block count and block size) and runs every
+sweep inside one kernel launch, instances dispatched largest-first from a
+device work queue.  ``BatchPlan`` keeps the outputs, workspace and uploaded
+descriptors so repeated runs cost one memset and one launch (capturable in a
+CUDA graph).
+"""
+
+import ctypes
+
+import numpy as np
+
+from .. import _lib
+from . import _device as dev
+
+
+class BatchPlan:
+    """Outputs, workspace and descriptors of one batch, reusable across runs.
+
+    ``instances``: sequence of ``(A_diag, A_upper, A_lower)`` (torch CUDA
+    tensors or numpy arrays; one dtype for the batch, complex128 or float64).
+    ``outputs`` (optional): matching ``(G_diag, G_upper, G_lower)`` tensors to
+    write into instead of allocating.
+    """
+
+    def __init__(self, instances, sym_mat=False, save_off_diag=True, precision="fp64", outputs=None,
+                 device=None):
+        torch = dev._torch()
+        self.lib = _lib.load()
+        if len(instances) == 0:
+            raise ValueError("empty batch")
+        tdt = dev.torch_dtype(instances[0][0])
+        self.code = _lib.dtype_code(tdt)
+        if self.code not in (_lib.C128, _lib.F64):
+            raise TypeError("batched RGF takes complex128 or float64 instances")
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.flags = (_lib.SYM if sym_mat else 0) | (_lib.SAVE_OFFDIAG if save_off_diag else 0)
+        if precision == "mixed":
+            self.flags |= _lib.PREC_MIXED
+        self.save_off_diag = save_off_diag
+        self.inputs, self.outputs, self.shapes = [], [], []
+        descs = (_lib.BatchDesc * len(instances))()
+        for k, inst in enumerate(instances):
+            d, u, l = inst
+            d = dev.to_device(d, tdt)
+            n, b = int(d.shape[0]), int(d.shape[1])
+            if d.dim() != 3 or d.shape[2] != b:
+                raise ValueError("instance %d: A_diag must be (n, b, b)" % k)
+            if n > 1:
+                u = dev.to_device(u, tdt)
+                l = dev.to_device(l, tdt)
+                if tuple(u.shape) != (n - 1, b, b) or tuple(l.shape) != (n - 1, b, b):
+                    raise ValueError("instance %d: off-diagonal blocks must be (%d, %d, %d)" % (k, n - 1, b, b))
+            else:
+                u = l = None
+            if outputs is not None:
+                Gd, Gu, Gl = outputs[k]
+            else:
+                Gd = torch.empty((n, b, b), dtype=tdt, device=d.device)
+                Gu = torch.empty((n - 1, b, b), dtype=tdt, device=d.device)
+                Gl = torch.empty((n - 1, b, b), dtype=tdt, device=d.device)
+            self.inputs.append((d, u, l))
+            self.outputs.append((Gd, Gu, Gl))
+            self.shapes.append((n, b))
+            descs[k] = _lib.BatchDesc(d.data_ptr(), u.data_ptr() if u is not None else None,
+                                      l.data_ptr() if l is not None else None, Gd.data_ptr(),
+                                      Gu.data_ptr() if (save_off_diag and n > 1) else None,
+                                      Gl.data_ptr() if (save_off_diag and n > 1) else None, n, b)
+        self.descs = descs
+        self.device = self.inputs[0][0].device
+        nbytes = self.lib.sinvb_rgf_batched_workspace_size(ctypes.cast(descs, ctypes.c_void_p), len(descs),
+                                                           self.code, self.flags)
+        with torch.cuda.device(self.device):
+            self.ws = dev.workspace(nbytes, self.device)
+            self.status_dev = torch.zeros(len(descs), dtype=torch.int32, device=self.device)
+        self.uploaded = False
+
+    @property
+    def count(self):
+        return len(self.shapes)
+
+    def run(self, stream=None):
+        """Enqueue the batch (first run uploads descriptors, later runs only launch)."""
+        torch = dev._torch()
+        with torch.cuda.device(self.device):
+            h = dev.stream_handle(stream)
+            if not self.uploaded:
+                fn = self.lib.sinvb_rgf_batched_z if self.code == _lib.C128 else self.lib.sinvb_rgf_batched_d
+                rc = fn(ctypes.cast(self.descs, ctypes.c_void_p), len(self.descs), self.flags, dev.ptr(self.ws),
+                        self.ws.numel(), dev.ptr(self.status_dev), h)
+                _lib.check(rc, "sinvb_rgf_batched")
+                self.uploaded = True
+            else:
+                fn = self.lib.sinvb_rgf_batched_rerun_z if self.code == _lib.C128 else \
+                    self.lib.sinvb_rgf_batched_rerun_d
+                _lib.check(fn(dev.ptr(self.ws), h), "sinvb_rgf_batched_rerun")
+
+    def statuses(self):
+        """Per-instance device status (synchronises)."""
+        return self.status_dev.cpu().numpy()
+
+    def check(self):
+        st = self.statuses()
+        bad = np.nonzero(st)[0]
+        if bad.size:
+            k = int(bad[0])
+            if st[k] == _lib.STATUS_PIVOT:
+                raise np.linalg.LinAlgError(
+                    "rgf_batched: zero or non-finite pivot in instance %d (%d instances failed)" % (k, bad.size))
+            raise RuntimeError("rgf_batched: instance %d status %d" % (k, st[k]))
+
+    def results(self, like=None):
+        out = []
+        for (Gd, Gu, Gl) in self.outputs:
+            if not self.save_off_diag:
+                Gu.fill_(float("nan"))
+                Gl.fill_(float("nan"))
+            if like is not None and not dev.is_torch(like):
+                out.append((Gd.cpu().numpy(), Gu.cpu().numpy(), Gl.cpu().numpy()))
+            else:
+                out.append((Gd, Gu, Gl))
+        return out
+
+
+def rgf_batched(instances, sym_mat=False, save_off_diag=True, precision="fp64", check=True, stream=None):
+    """Selected inversion of every ``(A_diag, A_upper, A_lower)`` in ``instances``.
+
+    Returns a list of ``(G_diag, G_upper, G_lower)`` in the input order, numpy
+    when the inputs are numpy.  ``check`` synchronises and raises
+    ``numpy.linalg.LinAlgError`` naming the first instance with a zero or
+    non-finite pivot.
+    """
+    plan = BatchPlan(instances, sym_mat, save_off_diag, precision)
+    plan.run(stream)
+    if check:
+        plan.check()
+    return plan.results(like=instances[0][0])

@@ -39,7 +39,7 @@ struct GjShared {
 // Returns false (and reports) on a zero / non-finite pivot; the block then
 // holds non-finite values.
 template <class T>
-__device__ bool cta_gj_invert(T* a, int lda, int m, WsHeader* hdr, int detail, void* smem_raw) {
+__device__ bool cta_gj_invert(T* a, int lda, int m, int* status, void* smem_raw) {
   GjShared<T>& sh = *reinterpret_cast<GjShared<T>*>(smem_raw);
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
   T v[4][4];
@@ -68,7 +68,7 @@ __device__ bool cta_gj_invert(T* a, int lda, int m, WsHeader* hdr, int detail, v
     const T ip = sh.pinv[buf];
     if (tid == 0 && !bad && !pivot_ok(sh.rowbuf[buf][k])) {
       bad = true;
-      report(hdr, SINVB_STATUS_PIVOT, detail);
+      report(status, SINVB_STATUS_PIVOT);
     }
     T rk[4], ck[4];
 #pragma unroll
@@ -137,9 +137,9 @@ __host__ __device__ inline size_t invert_side_elems(int m) { return m > kPanel ?
 // visible to the whole team (the caller synchronised before; this function
 // synchronises after).  Returns false when a team barrier gave up.
 template <class T, int BM, int BN, class Team>
-__device__ bool team_invert(Team& team, T* a, int lda, int m, T* W, WsHeader* hdr, int detail, T* smem) {
+__device__ bool team_invert(Team& team, T* a, int lda, int m, T* W, int* status, T* smem) {
   if (m <= kPanel) {
-    if (team.rank() == 0) cta_gj_invert<T>(a, lda, m, hdr, detail, smem);
+    if (team.rank() == 0) cta_gj_invert<T>(a, lda, m, status, smem);
     return team.sync();
   }
   const int np = (m + kPanel - 1) / kPanel;
@@ -148,7 +148,7 @@ __device__ bool team_invert(Team& team, T* a, int lda, int m, T* W, WsHeader* hd
     const int K0 = p * kPanel, kb = min(kPanel, m - K0);
     T* Dinv = a + (size_t)K0 * lda + K0;
     // (1) invert the pivot block; copy back the previous column panel
-    if (team.rank() == 0) cta_gj_invert<T>(Dinv, lda, kb, hdr, detail, smem);
+    if (team.rank() == 0) cta_gj_invert<T>(Dinv, lda, kb, status, smem);
     if (prevK0 >= 0) {
       // rows above and below the previous panel
       team_copy<T>(team, prevK0, prevkb, W, kPanel, a + prevK0, lda);

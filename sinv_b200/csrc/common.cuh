@@ -65,17 +65,25 @@ __device__ __forceinline__ bool pivot_ok(cplx p) {
 // Workspace header: first 256 bytes of every workspace.
 // ---------------------------------------------------------------------------
 struct WsHeader {
-  int status;                 // SINVB_OK or SINVB_STATUS_*
-  int status_detail;          // block index / location of the first failure
+  int status;                 // SINVB_OK or SINVB_STATUS_* (first failure of the call)
+  int reserved;
   unsigned int barrier_count; // grid-team barrier arrivals
   unsigned int queue_head;    // batched work queue
-  unsigned int pad[60];
+  // batched launches: written by the upload, read by the persistent kernel
+  int count;                  // instances
+  unsigned int flags;
+  unsigned int nslots;        // per-CTA scratch slots
+  unsigned int pad0;
+  unsigned long long slot_bytes;
+  unsigned long long desc_offset;
+  unsigned long long slots_offset;
+  int* inst_status;           // caller's per-instance status array (may be null)
+  unsigned int pad[48];
 };
 static_assert(sizeof(WsHeader) == 256, "header is 256 bytes");
 
-__device__ __forceinline__ void report(WsHeader* h, int code, int detail) {
-  if (atomicCAS(&h->status, 0, code) == 0) h->status_detail = detail;
-}
+// First failure wins; later ones keep the first code.
+__device__ __forceinline__ void report(int* status, int code) { atomicCAS(status, 0, code); }
 
 // Iteration bound of every spin-wait: ~2^24 polls with backoff is well over a
 // second on B200 and far below any watchdog.
@@ -135,12 +143,13 @@ struct TeamGrid {
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(&hdr->barrier_count) : "memory");
         if (seen >= target) break;
         if (++spins > kSpinLimit) {
-          report(hdr, SINVB_STATUS_TIMEOUT, -1);
+          report(&hdr->status, SINVB_STATUS_TIMEOUT);
           good = 0;
           break;
         }
         if (spins > 64) __nanosleep(32);
       }
+      __threadfence();
       ok = good;
     }
     __syncthreads();

@@ -120,6 +120,7 @@ static int run_rgf(const T* diag, const T* upper, const T* lower, int n, int b, 
   p.T1 = reinterpret_cast<T*>(ws + L.T1);
   p.Winv = reinterpret_cast<T*>(ws + L.Winv);
   p.hdr = reinterpret_cast<WsHeader*>(ws);
+  p.status = &p.hdr->status;
   p.n = n;
   p.b = b;
   p.flags = flags;

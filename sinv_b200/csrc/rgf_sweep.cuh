@@ -41,7 +41,8 @@ struct RgfParams {
   T* T0;   // b*b
   T* T1;   // b*b
   T* Winv; // invert_side_elems(b)
-  WsHeader* hdr;
+  WsHeader* hdr;   // grid-team barrier counter (unused by other teams)
+  int* status;     // device status word of this matrix
   int n, b;
   unsigned flags;
 };
@@ -56,7 +57,7 @@ __device__ void rgf_sweep(Team& team, const RgfParams<T>& p, T* smem) {
   // g_0 = A_00^{-1}
   team_copy<T>(team, b, b, p.diag, b, p.Gd, b);
   if (!team.sync()) return;
-  if (!team_invert<T, BM, BN>(team, p.Gd, b, b, p.Winv, p.hdr, 0, smem)) return;
+  if (!team_invert<T, BM, BN>(team, p.Gd, b, b, p.Winv, p.status, smem)) return;
 
   for (int i = 1; i < n; i++) {
     const T* g = p.Gd + (i - 1) * bb;
@@ -75,7 +76,7 @@ __device__ void rgf_sweep(Team& team, const RgfParams<T>& p, T* smem) {
       team_gemm<T, BM, BN>(team, &op, 1, smem);
     }
     if (!team.sync()) return;
-    if (!team_invert<T, BM, BN>(team, p.Gd + i * bb, b, b, p.Winv, p.hdr, i, smem)) return;
+    if (!team_invert<T, BM, BN>(team, p.Gd + i * bb, b, b, p.Winv, p.status, smem)) return;
   }
 
   T* prevT = nullptr;
