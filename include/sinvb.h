@@ -138,6 +138,25 @@ int sinvb_rgf_batched_d(const sinvb_batch_desc* descs, int count, unsigned flags
 int sinvb_rgf_batched_rerun_z(void* workspace, sinvb_stream_t stream);
 int sinvb_rgf_batched_rerun_d(void* workspace, sinvb_stream_t stream);
 
+/* ---- allocation-free variant ------------------------------------------------ */
+/*
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they call (inside a stream capture whose graph must hold no
+ * allocation nodes, inside an allocator hook or host callback, or in a
+ * plugin whose host application owns all device memory): the single-matrix
+ * complex128 RGF of sinvb_rgf_z with the scratch in a static device array
+ * owned by the library (131,328 bytes, held by every GPU that loads the
+ * library until exit), so only inputs and outputs are passed.
+ * Limits: b <= 64; SINVB_SAVE_OFFDIAG required when n > 1; flags other than
+ * SINVB_SYM / SINVB_SAVE_OFFDIAG rejected (SINVB_EINVAL).  ``status``
+ * (optional, device, one int) receives the device status.  The first call on
+ * a device looks up the array's address: make it before any stream capture.
+ * All calls share the array, so calls that overlap on the GPU race.
+ */
+int sinvb_rgf_z_noalloc(const void* diag, const void* upper, const void* lower, int n, int b,
+                        unsigned flags, void* G_diag, void* G_upper, void* G_lower, int* status,
+                        sinvb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -49,6 +49,7 @@ SIGNATURES = {
     "sinvb_rgf_batched_d": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp]),
     "sinvb_rgf_batched_rerun_z": (_i, [_vp, _vp]),
     "sinvb_rgf_batched_rerun_d": (_i, [_vp, _vp]),
+    "sinvb_rgf_z_noalloc": (_i, [_vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _vp]),
 }
 
 PREC_FP64 = 0
