@@ -44,16 +44,22 @@ def parse():
     ap.add_argument("--impl", default="sinvb", choices=["sinvb", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--count", type=int, default=512)
-    ap.add_argument("--wave-gb", type=float, default=0.0, help="input bytes per wave (0: from free memory)")
+    ap.add_argument("--shape", default=None, help="n,b: uniform batch of that shape instead of the energy batch")
+    ap.add_argument("--wave-gb", type=float, default=0.0, help="input GB per wave (0: as much as HBM holds)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
     return ap.parse_args()
 
 
 # --------------------------------------------------------------------------- helpers
-def batch_spec(count, rank):
+def batch_spec(count, rank, shape=None):
+    """Instances (E, n, b, seed) of this rank's batch: the energy batch, or with
+    ``shape`` = (n, b) a uniform batch of that shape (small profiling cases)."""
     from sinv_b200 import workloads
     spec = workloads.energy_batch_spec(count=count)
+    if shape is not None:
+        spec = [(e, shape[0], shape[1], s) for (e, _, _, s) in spec]
     if rank:
         spec = [(e, n, b, s + 100000 * rank) for (e, n, b, s) in spec]
     return spec
@@ -208,7 +214,8 @@ def cpu_baseline(spec, reps=1):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    spec = batch_spec(args.count, 0)
+    shape = tuple(int(x) for x in args.shape.split(",")) if args.shape else None
+    spec = batch_spec(args.count, 0, shape)
     vals = []
     for step in range(args.warmup + args.steps):
         cb = cpu_baseline(spec)
@@ -234,25 +241,25 @@ def run_sinvb(args, rank, world, local_rank):
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    spec = batch_spec(args.count, rank)
+    shape = tuple(int(x) for x in args.shape.split(",")) if args.shape else None
+    spec = batch_spec(args.count, rank, shape)
     peak = fp64_peak_tflops(torch)
 
     free, _ = torch.cuda.mem_get_info()
+    # In place (results over the inputs): the whole batch fits in HBM as one
+    # wave; the per-CTA scratch slots need ~3 GB more.
     if args.wave_gb > 0:
         budget = int(args.wave_gb * 1e9 / 16)
     else:
-        budget = int(0.40 * free / 16)       # inputs; outputs take as much again
+        budget = int((free - 6e9) / 16)
     max_inst = max(in_elems(n, b) for (_, n, b, _) in spec)
     budget = max(budget, max_inst)
     waves = make_waves(spec, budget)
     pool_elems = max(sum(in_elems(spec[k][1], spec[k][2]) for k in w) for w in waves)
     pin = torch.empty(pool_elems, dtype=torch.complex128, device=dev)
-    pout = torch.empty(pool_elems, dtype=torch.complex128, device=dev)
     plans = []
     for w in waves:
-        ins = carve(pin, spec, w)
-        outs = carve(pout, spec, w)
-        plans.append(BatchPlan(ins, outputs=outs, precision=args.precision))
+        plans.append(BatchPlan(carve(pin, spec, w), precision=args.precision, inplace=True))
     flops = [sum(workloads.rgf_flops(spec[k][1], spec[k][2]) for k in w) for w in waves]
 
     def generate(wi):
@@ -261,38 +268,32 @@ def run_sinvb(args, rank, world, local_rank):
             workloads.tight_binding_device(n, b, e, s, device=dev, out=(d, u, l))
 
     stream = torch.cuda.current_stream()
-    resident = len(waves) == 1
-    if resident:
-        generate(0)
     clocks = Clocks(local_rank) if rank == 0 else None
     step_ms, kern_ms, kern_flops = [], [], []
     for step in range(args.warmup + args.steps):
         timed = step >= args.warmup
         if timed and step == args.warmup and clocks:
             clocks.start()
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
         total = 0.0
         for wi, plan in enumerate(plans):
-            if not resident:
-                generate(wi)
-                torch.cuda.synchronize()
+            generate(wi)           # in place: every launch starts from fresh inputs (untimed)
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
             e0.record(stream)
             plan.run(stream)
             e1.record(stream)
             e1.synchronize()
             ms = e0.elapsed_time(e1)
+            if world > 1:
+                t = torch.tensor([ms], dtype=torch.float64, device=dev)
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                ms = float(t.item())
             total += ms
             if timed:
                 kern_ms.append(ms)
                 kern_flops.append(flops[wi])
-        torch.cuda.synchronize()
-        if world > 1:
-            t = torch.tensor([total], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total = float(t.item())
         if timed:
             step_ms.append(total)
     clk = clocks.stop() if clocks else None
@@ -307,13 +308,15 @@ def run_sinvb(args, rank, world, local_rank):
     if args.precision != "fp64":
         acc = "not measured"
 
+    workload = WORKLOAD if shape is None else "uniform_%dx(n=%d,b=%d)" % (args.count, shape[0], shape[1])
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "c128" if args.precision == "fp64" else "c128 (mixed products)",
            "data": "synthetic",
-           "config": {"workload": WORKLOAD, "count": args.count, "block_sizes": [64, 128, 256, 512],
+           "config": {"workload": workload, "count": args.count, "block_sizes": [64, 128, 256, 512],
                       "n_range": [16, 128], "precision": args.precision, "path": "batched persistent",
                       "waves": len(waves), "wave_input_gb": round(pool_elems * 16 / 1e9, 2),
+                      "in_place": True,
                       "l2": "inputs larger than L2 in every wave", "parallelism": "replicas%d" % world},
            "gpu_launches": len(plans) * args.steps,
            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -325,17 +328,35 @@ def run_sinvb(args, rank, world, local_rank):
     if acc is not None:
         out["rel_err_vs_fp64"] = acc
 
-    del pin, pout, plans
+    # the plain per-matrix FP64 path (one library call per instance, the whole
+    # GPU on each matrix) over the same batch, one pass, same in-place inputs
+    if not args.no_plain:
+        plain_ms = 0.0
+        for wi, plan in enumerate(plans):
+            generate(wi)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+            e0.record(stream)
+            for (d, u, l) in plan.inputs:
+                rgf.rgf_blocks(d, u, l, check=False, overwrite_a=True)
+            e1.record(stream)
+            e1.synchronize()
+            plain_ms += e0.elapsed_time(e1)
+        plain = args.count / (plain_ms * 1e-3)
+        out["vs_plain_fp64"] = {"batched": value / world, "plain_per_matrix_fp64": plain,
+                                "ratio": value / world / plain, "sample": "the whole batch, one pass"}
+
+    del pin, plans, plan   # `plan` (loop variable) holds views of the pool too
     torch.cuda.empty_cache()
-    # e2e and batched-vs-plain on a stratified sample (every 16th instance)
+    # e2e on a stratified sample (every 16th instance)
     if not args.no_e2e:
-        out["e2e"], out["vs_plain_fp64"] = e2e_and_plain(torch, spec, args, dev, world)
+        out["e2e"] = e2e_sample(torch, spec, args, dev, world)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(spec)
     return out
 
 
-def e2e_and_plain(torch, spec, args, dev, world):
+def e2e_sample(torch, spec, args, dev, world):
     """End-to-end (pinned host buffers, copies inside the timed region) through the
     public BatchPlan API, and the plain per-matrix FP64 path on the same sample."""
     import torch.distributed as dist
@@ -372,8 +393,8 @@ def e2e_and_plain(torch, spec, args, dev, world):
             times.append(e0.elapsed_time(e1))
     plan.check()
     ms = statistics.mean(times)
-    # device-only batched and plain per-matrix FP64 on the same sample
-    dev_t, plain_t = [], []
+    # the same sample device-only, for comparison with the e2e figure
+    dev_t = []
     for step in range(2):
         e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
         e0.record(stream)
@@ -381,23 +402,14 @@ def e2e_and_plain(torch, spec, args, dev, world):
         e1.record(stream)
         e1.synchronize()
         dev_t.append(e0.elapsed_time(e1))
-        e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
-        e0.record(stream)
-        for (d, u, l) in ins:
-            rgf.rgf_blocks(d, u, l, check=False)
-        e1.record(stream)
-        e1.synchronize()
-        plain_t.append(e0.elapsed_time(e1))
     bytes_step = tot * 16
     e2e = {"value": len(idx) * world / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bytes_step,
            "d2h_bytes_per_step": bytes_step,
-           "sample": "every 16th instance of the batch (%d instances, %.1f GB in)" % (len(idx), bytes_step / 1e9),
+           "sample": "every 16th instance of the batch (%d instances, %.1f GB in), pinned host buffers, "
+                     "copies inside the timed region" % (len(idx), bytes_step / 1e9),
            "device_only_value_same_sample": len(idx) / (min(dev_t) * 1e-3)}
-    vs = {"sample": e2e["sample"], "batched": len(idx) / (min(dev_t) * 1e-3),
-          "plain_per_matrix_fp64": len(idx) / (min(plain_t) * 1e-3)}
-    vs["ratio"] = vs["batched"] / vs["plain_per_matrix_fp64"]
     del host_in, host_out, pin_dev, pout_dev, plan
-    return e2e, vs
+    return e2e
 
 
 def main():

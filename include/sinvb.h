@@ -53,6 +53,11 @@ typedef struct CUstream_st* sinvb_stream_t; /* == cudaStream_t */
  * small blocks; by default the library picks the team from b */
 #define SINVB_FORCE_GRID 4u
 #define SINVB_FORCE_CTA 8u
+/* overwrite the inputs with the results: G_diag -> diag, G_upper -> upper,
+ * G_lower -> lower (the G_* arguments are ignored; requires SAVE_OFFDIAG).
+ * Halves the memory of a call; the reference never does this (rgf.py:41
+ * copies), so the Python layer uses it only when asked. */
+#define SINVB_INPLACE 16u
 
 /* ---- element type codes --------------------------------------------------- */
 #define SINVB_C128 0 /* complex double */
@@ -94,6 +99,53 @@ int sinvb_rgf_s(const void* diag, const void* upper, const void* lower, int n, i
  * reset by the next call that uses the workspace.
  */
 int sinvb_workspace_status(const void* workspace, sinvb_stream_t stream, int* status);
+
+/* ---- adjoint (reverse mode) of the RGF sweeps ------------------------------------ */
+/*
+ * No reference counterpart (the reference has no gradients); the adjoint of
+ * src/sinv/algorithms/rgf/rgf.py:44-62.  The forward call saves checkpoints
+ * g_{s*c-1} (c = ceil(sqrt(n)), sinvb_rgf_checkpoints gives c and the count)
+ * so the adjoint recomputes the left-connected blocks instead of storing all
+ * of them.  Requires SINVB_SAVE_OFFDIAG.  Upstream adjoints bG_* follow the
+ * torch convention (dL/dG* for complex, dL/dG for real); bG_upper / bG_lower
+ * may be NULL (zero).  Outputs aD (n blocks), aU, aL (n-1 blocks): dL/dA* on
+ * the tridiagonal pattern.
+ */
+int sinvb_rgf_checkpoints(int n, int* every, int* count);
+int sinvb_rgf_forward_ckpt_z(const void* diag, const void* upper, const void* lower, int n, int b,
+                             unsigned flags, void* G_diag, void* G_upper, void* G_lower, void* checkpoints,
+                             int every, void* workspace, size_t workspace_bytes, sinvb_stream_t stream);
+int sinvb_rgf_forward_ckpt_d(const void* diag, const void* upper, const void* lower, int n, int b,
+                             unsigned flags, void* G_diag, void* G_upper, void* G_lower, void* checkpoints,
+                             int every, void* workspace, size_t workspace_bytes, sinvb_stream_t stream);
+size_t sinvb_rgf_adjoint_workspace_size(int n, int b, int dtype, unsigned flags);
+int sinvb_rgf_adjoint_z(const void* diag, const void* upper, const void* lower, const void* G_diag,
+                        const void* G_upper, const void* G_lower, const void* bG_diag, const void* bG_upper,
+                        const void* bG_lower, const void* checkpoints, int every, int n, int b, unsigned flags,
+                        void* aD, void* aU, void* aL, void* workspace, size_t workspace_bytes,
+                        sinvb_stream_t stream);
+int sinvb_rgf_adjoint_d(const void* diag, const void* upper, const void* lower, const void* G_diag,
+                        const void* G_upper, const void* G_lower, const void* bG_diag, const void* bG_upper,
+                        const void* bG_lower, const void* checkpoints, int every, int n, int b, unsigned flags,
+                        void* aD, void* aU, void* aL, void* workspace, size_t workspace_bytes,
+                        sinvb_stream_t stream);
+
+/* ---- BCR: block cyclic reduction on the whole GPU ------------------------------ */
+/*
+ * Replaces ``bcr_serial(A, blocksize)`` of
+ * src/sinv/algorithms/bcr/bcr_serial.py:19-62 (reduce :66-216, root inverse
+ * :220-249, production :253-466; padding and index sets of
+ * src/sinv/algorithms/bcr/bcr_utils.py:17-129) in block-array form: the
+ * G_ii, G_{i,i+1}, G_{i+1,i} blocks the reference's dense result holds.  The
+ * rows of each reduction / production level run in parallel on every SM.
+ */
+size_t sinvb_bcr_workspace_size(int n, int b, int dtype, unsigned flags);
+int sinvb_bcr_z(const void* diag, const void* upper, const void* lower, int n, int b, unsigned flags,
+                void* G_diag, void* G_upper, void* G_lower, void* workspace, size_t workspace_bytes,
+                sinvb_stream_t stream);
+int sinvb_bcr_d(const void* diag, const void* upper, const void* lower, int n, int b, unsigned flags,
+                void* G_diag, void* G_upper, void* G_lower, void* workspace, size_t workspace_bytes,
+                sinvb_stream_t stream);
 
 /* ---- batched RGF: many independent matrices in one persistent launch ------- */
 /*

@@ -26,6 +26,7 @@ SYM = 1
 SAVE_OFFDIAG = 2
 FORCE_GRID = 4
 FORCE_CTA = 8
+INPLACE = 16
 
 C128, F64, C64, F32 = 0, 1, 2, 3
 
@@ -50,6 +51,15 @@ SIGNATURES = {
     "sinvb_rgf_batched_rerun_z": (_i, [_vp, _vp]),
     "sinvb_rgf_batched_rerun_d": (_i, [_vp, _vp]),
     "sinvb_rgf_z_noalloc": (_i, [_vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _vp]),
+    "sinvb_rgf_checkpoints": (_i, [_i, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "sinvb_rgf_forward_ckpt_z": (_i, [_vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _i, _vp, _sz, _vp]),
+    "sinvb_rgf_forward_ckpt_d": (_i, [_vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _i, _vp, _sz, _vp]),
+    "sinvb_rgf_adjoint_workspace_size": (_sz, [_i, _i, _i, _u]),
+    "sinvb_rgf_adjoint_z": (_i, [_vp] * 10 + [_i, _i, _i, _u, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "sinvb_rgf_adjoint_d": (_i, [_vp] * 10 + [_i, _i, _i, _u, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "sinvb_bcr_workspace_size": (_sz, [_i, _i, _i, _u]),
+    "sinvb_bcr_z": (_i, _RGF_ARGS),
+    "sinvb_bcr_d": (_i, _RGF_ARGS),
 }
 
 PREC_FP64 = 0

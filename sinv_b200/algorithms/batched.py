@@ -24,11 +24,15 @@ class BatchPlan:
     ``instances``: sequence of ``(A_diag, A_upper, A_lower)`` (torch CUDA
     tensors or numpy arrays; one dtype for the batch, complex128 or float64).
     ``outputs`` (optional): matching ``(G_diag, G_upper, G_lower)`` tensors to
-    write into instead of allocating.
+    write into instead of allocating.  ``inplace=True`` overwrites the input
+    tensors with the results instead (torch CUDA inputs only; halves the
+    memory, which lets a batch larger than half of HBM run as one launch).
+    ``team="cta"`` runs every instance on a single CTA; by default large
+    blocks get teams of 2-8 CTAs.
     """
 
     def __init__(self, instances, sym_mat=False, save_off_diag=True, precision="fp64", outputs=None,
-                 device=None):
+                 device=None, inplace=False, team=None):
         torch = dev._torch()
         self.lib = _lib.load()
         if len(instances) == 0:
@@ -42,6 +46,16 @@ class BatchPlan:
         self.flags = (_lib.SYM if sym_mat else 0) | (_lib.SAVE_OFFDIAG if save_off_diag else 0)
         if precision == "mixed":
             self.flags |= _lib.PREC_MIXED
+        if inplace:
+            if not save_off_diag:
+                raise ValueError("inplace requires save_off_diag=True")
+            if not all(dev.is_torch(x) and x.is_cuda for x in instances[0] if x is not None):
+                raise TypeError("inplace takes torch CUDA tensors")
+            self.flags |= _lib.INPLACE
+        if team == "cta":
+            self.flags |= _lib.FORCE_CTA
+        elif team is not None:
+            raise ValueError("team must be None or 'cta'")
         self.save_off_diag = save_off_diag
         self.inputs, self.outputs, self.shapes = [], [], []
         descs = (_lib.BatchDesc * len(instances))()
@@ -58,7 +72,12 @@ class BatchPlan:
                     raise ValueError("instance %d: off-diagonal blocks must be (%d, %d, %d)" % (k, n - 1, b, b))
             else:
                 u = l = None
-            if outputs is not None:
+            if inplace:
+                if n > 1 and (u.data_ptr() != inst[1].data_ptr() or l.data_ptr() != inst[2].data_ptr()) or \
+                        d.data_ptr() != inst[0].data_ptr():
+                    raise ValueError("inplace needs contiguous inputs of the batch dtype")
+                Gd, Gu, Gl = d, u if u is not None else d[:0], l if l is not None else d[:0]
+            elif outputs is not None:
                 Gd, Gu, Gl = outputs[k]
             else:
                 Gd = torch.empty((n, b, b), dtype=tdt, device=d.device)

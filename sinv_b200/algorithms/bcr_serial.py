@@ -1,0 +1,94 @@
+"""Block cyclic reduction selected inversion on the GPU -- drop-in for the
+reference's ``sinv.algorithms.bcr_s`` (``src/sinv/algorithms/bcr/bcr_serial.py``).
+
+``bcr_serial(A, blocksize)`` takes the dense matrix like the reference
+(``bcr_serial.py:19-62``) and returns a dense G holding the block-tridiagonal
+part of the inverse (G_ii, G_{i,i+1}, G_{i+1,i}), zero elsewhere; the
+reference's dense output additionally carries the intermediate blocks of its
+production tree, which are not part of the selected inverse.
+``bcr_blocks(A_diag, A_upper, A_lower)`` is the block-array form.
+
+complex128 and float64 run natively; complex64 / float32 inputs are computed
+in FP64 and rounded back.  Everything runs in ``libsinvb.so``.
+"""
+
+import numpy as np
+
+from .. import _lib
+from . import _device as dev
+
+
+def bcr_blocks(A_diag, A_upper, A_lower, check=True, stream=None):
+    """Selected inversion by BCR.  Returns ``(G_diag, G_upper, G_lower)``."""
+    lib = _lib.load()
+    torch = dev._torch()
+    in_dt = dev.torch_dtype(A_diag)
+    wide = {torch.complex64: torch.complex128, torch.float32: torch.float64}.get(in_dt, in_dt)
+    code = _lib.dtype_code(wide)
+    if code not in (_lib.C128, _lib.F64):
+        raise TypeError("unsupported dtype %s" % in_dt)
+    d = dev.to_device(A_diag, wide)
+    if d.dim() != 3 or d.shape[1] != d.shape[2]:
+        raise ValueError("A_diag must be (n, b, b), got %s" % (tuple(d.shape),))
+    n, b = int(d.shape[0]), int(d.shape[1])
+    if n > 1:
+        u = dev.to_device(A_upper, wide)
+        l = dev.to_device(A_lower, wide)
+        for name, t in (("A_upper", u), ("A_lower", l)):
+            if tuple(t.shape) != (n - 1, b, b):
+                raise ValueError("%s must be (%d, %d, %d), got %s" % (name, n - 1, b, b, tuple(t.shape)))
+    else:
+        u = l = None
+    Gd = torch.empty((n, b, b), dtype=wide, device=d.device)
+    Gu = torch.empty((n - 1, b, b), dtype=wide, device=d.device)
+    Gl = torch.empty((n - 1, b, b), dtype=wide, device=d.device)
+    with torch.cuda.device(d.device):
+        ws = dev.workspace(lib.sinvb_bcr_workspace_size(n, b, code, 0), d.device)
+        fn = lib.sinvb_bcr_z if code == _lib.C128 else lib.sinvb_bcr_d
+        rc = fn(dev.ptr(d), dev.ptr(u), dev.ptr(l), n, b, 0, dev.ptr(Gd), dev.ptr(Gu), dev.ptr(Gl), dev.ptr(ws),
+                ws.numel(), dev.stream_handle(stream))
+        _lib.check(rc, "sinvb_bcr")
+        if check:
+            dev.raise_for_status(dev.read_status(lib, ws, stream), "bcr_serial")
+    out = tuple(g.to(in_dt) if wide != in_dt else g for g in (Gd, Gu, Gl))
+    return tuple(dev.to_output(g, A_diag) for g in out)
+
+
+def bcr_serial(A, blocksize, **kw):
+    """Drop-in for ``bcr_serial(A, blocksize)`` (``bcr_serial.py:19-22``): dense in, dense out."""
+    is_t = dev.is_torch(A)
+    An = A if is_t else np.asarray(A)
+    N = An.shape[0]
+    b = int(blocksize)
+    if An.shape[0] != An.shape[1] or N % b:
+        raise ValueError("A must be square with a size divisible by blocksize")
+    n = N // b
+    if is_t:
+        blocks = An.reshape(n, b, n, b).permute(0, 2, 1, 3)
+        d = blocks[range(n), range(n)].contiguous()
+        u = blocks[range(n - 1), range(1, n)].contiguous() if n > 1 else None
+        l = blocks[range(1, n), range(n - 1)].contiguous() if n > 1 else None
+    else:
+        blocks = An.reshape(n, b, n, b).transpose(0, 2, 1, 3)
+        idx = np.arange(n)
+        d = np.ascontiguousarray(blocks[idx, idx])
+        u = np.ascontiguousarray(blocks[idx[:-1], idx[1:]]) if n > 1 else np.zeros((0, b, b), An.dtype)
+        l = np.ascontiguousarray(blocks[idx[1:], idx[:-1]]) if n > 1 else np.zeros((0, b, b), An.dtype)
+    Gd, Gu, Gl = bcr_blocks(d, u, l, **kw)
+    if is_t:
+        torch = dev._torch()
+        G = torch.zeros((N, N), dtype=Gd.dtype, device=Gd.device)
+        Gv = G.view(n, b, n, b).permute(0, 2, 1, 3)
+        for i in range(n):
+            Gv[i, i] = Gd[i]
+            if i < n - 1:
+                Gv[i, i + 1] = Gu[i]
+                Gv[i + 1, i] = Gl[i]
+        return G
+    G = np.zeros((N, N), dtype=Gd.dtype)
+    for i in range(n):
+        G[i * b:(i + 1) * b, i * b:(i + 1) * b] = Gd[i]
+        if i < n - 1:
+            G[i * b:(i + 1) * b, (i + 1) * b:(i + 2) * b] = Gu[i]
+            G[(i + 1) * b:(i + 2) * b, i * b:(i + 1) * b] = Gl[i]
+    return G

@@ -29,13 +29,15 @@ def _is_container(A):
 
 
 def rgf_blocks(A_diag, A_upper, A_lower, sym_mat=False, save_off_diag=True, check=True, stream=None,
-               team=None):
+               team=None, overwrite_a=False):
     """Block-array selected inversion.  Returns ``(G_diag, G_upper, G_lower)``.
 
     ``check`` synchronises and raises ``numpy.linalg.LinAlgError`` on a zero or
     non-finite pivot (the reference's ``np.linalg.inv`` failure mode).
     ``team`` forces the execution team: ``"cta"`` (one CTA walks the sweep) or
     ``"grid"`` (the whole GPU); by default the library picks from the block size.
+    ``overwrite_a`` (torch CUDA complex128/float64 inputs, ``save_off_diag``)
+    writes the results over the input tensors and returns them.
     """
     lib = _lib.load()
     tdt = dev.torch_dtype(A_diag)
@@ -62,9 +64,20 @@ def rgf_blocks(A_diag, A_upper, A_lower, sym_mat=False, save_off_diag=True, chec
         flags |= _lib.FORCE_CTA
     elif team is not None:
         raise ValueError("team must be None, 'cta' or 'grid'")
-    Gd = torch.empty((n, b, b), dtype=tdt, device=d.device)
-    Gu = torch.empty((n - 1, b, b), dtype=tdt, device=d.device)
-    Gl = torch.empty((n - 1, b, b), dtype=tdt, device=d.device)
+    if overwrite_a:
+        if not (dev.is_torch(A_diag) and A_diag.is_cuda and d.data_ptr() == A_diag.data_ptr()
+                and (n == 1 or (u.data_ptr() == A_upper.data_ptr() and l.data_ptr() == A_lower.data_ptr()))):
+            raise TypeError("overwrite_a takes contiguous torch CUDA tensors")
+        if not save_off_diag or code not in (_lib.C128, _lib.F64):
+            raise ValueError("overwrite_a needs save_off_diag=True and complex128 / float64")
+        flags |= _lib.INPLACE
+        Gd = d
+        Gu = u if u is not None else d[:0]
+        Gl = l if l is not None else d[:0]
+    else:
+        Gd = torch.empty((n, b, b), dtype=tdt, device=d.device)
+        Gu = torch.empty((n - 1, b, b), dtype=tdt, device=d.device)
+        Gl = torch.empty((n - 1, b, b), dtype=tdt, device=d.device)
     with torch.cuda.device(d.device):
         ws = dev.workspace(lib.sinvb_rgf_workspace_size(n, b, code, flags), d.device)
         fn = {_lib.C128: lib.sinvb_rgf_z, _lib.F64: lib.sinvb_rgf_d, _lib.C64: lib.sinvb_rgf_c,

@@ -13,12 +13,23 @@
 // Each CTA owns a scratch slot in the workspace (the T / side buffers of the
 // sweep, sized for the largest instance), reused instance after instance.
 #include <algorithm>
+#include <mutex>
+#include <unordered_map>
 #include <vector>
 
 #include "host_util.h"
 #include "rgf_sweep.cuh"
 
 namespace sinvb {
+
+// The instance count of the last upload into a workspace, kept host-side so a
+// re-run needs no device read (the kernel reads everything else from the
+// workspace header).
+static std::mutex g_count_mutex;
+static std::unordered_map<const void*, int>& count_table() {
+  static std::unordered_map<const void*, int> t;
+  return t;
+}
 
 template <class T>
 struct BatchEntry {
@@ -29,64 +40,99 @@ struct BatchEntry {
   T* Gu;
   T* Gl;
   int n, b;
-  int orig;  // index in the caller's descriptor array
-  int pad;
+  int orig;        // index in the caller's descriptor array
+  int team;        // CTAs working on this instance
+  int slot_start;  // first queue slot of this instance (entries are in queue order)
+  int pad[3];
 };
-static_assert(sizeof(BatchEntry<cplx>) == 64, "64-byte entries");
+static_assert(sizeof(BatchEntry<cplx>) == 80, "80-byte entries");
 
+// Per-instance meeting point of its team (64 bytes apart).
+struct ItemArea {
+  unsigned counter;  // team barrier arrivals
+  int status;        // device status of the instance
+  unsigned char* scratch;  // scratch slot of the team's rank-0 CTA
+  unsigned pad[12];
+};
+static_assert(sizeof(ItemArea) == 64, "64-byte item areas");
+
+// Persistent: every CTA repeatedly takes one queue slot.  Slot s belongs to the
+// instance k with slot_start[k] <= s < slot_start[k] + team[k], with rank
+// s - slot_start[k] in that instance's team.  Slots are handed out in order,
+// so a team completes as soon as its last member frees up; with teams sized
+// by block size (large blocks first) members mostly arrive together.  Every
+// CTA of the launch is resident (cooperative launch), so each team wait ends.
 template <class T>
 __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char* ws) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* smem = reinterpret_cast<T*>(smem_raw);
   WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
   const BatchEntry<T>* entries = reinterpret_cast<const BatchEntry<T>*>(ws + hdr->desc_offset);
+  ItemArea* items = reinterpret_cast<ItemArea*>(ws + hdr->items_offset);
   if (blockIdx.x >= hdr->nslots) return;
-  unsigned char* slot = ws + hdr->slots_offset + (size_t)blockIdx.x * hdr->slot_bytes;
+  unsigned char* my_slot = ws + hdr->slots_offset + (size_t)blockIdx.x * hdr->slot_bytes;
   const int count = hdr->count;
+  const int total_slots = hdr->total_slots;
   const unsigned flags = hdr->flags;
   const bool save = flags & SINVB_SAVE_OFFDIAG;
-  __shared__ int next;
-  __shared__ int inst_status;
-  TeamCta team;
+  const bool inplace = flags & SINVB_INPLACE;
+  __shared__ int sh_slot;
   while (true) {
-    if (threadIdx.x == 0) {
-      next = (int)atomicAdd(&hdr->queue_head, 1u);
-      inst_status = 0;
-    }
+    if (threadIdx.x == 0) sh_slot = (int)atomicAdd(&hdr->queue_head, 1u);
     __syncthreads();
-    const int k = next;
-    if (k >= count) return;
+    const int s = sh_slot;
+    __syncthreads();  // sh_slot is rewritten by the next dequeue
+    if (s >= total_slots) return;
+    int lo = 0, hi = count - 1;  // last entry with slot_start <= s
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (entries[mid].slot_start <= s) lo = mid; else hi = mid - 1;
+    }
+    const int k = lo;
     const BatchEntry<T> e = entries[k];
+    ItemArea* item = items + k;
+    const int rank = s - e.slot_start;
+    if (rank == 0 && threadIdx.x == 0) {
+      item->scratch = my_slot;
+      __threadfence();
+    }
+    TeamDyn team{&item->counter, &item->status, rank, e.team, 0u};
+    if (!team.sync()) continue;  // formation: the rank-0 scratch pointer is visible after this
+    unsigned char* slot = *((unsigned char* volatile*)&item->scratch);
     const size_t bb = (size_t)e.b * e.b;
     RgfParams<T> p;
     p.diag = e.diag;
     p.upper = e.upper;
     p.lower = e.lower;
-    p.Gd = e.Gd;
-    p.Gu = e.Gu;
-    p.Gl = e.Gl;
-    T* s = reinterpret_cast<T*>(slot);
-    p.T0 = s;
-    p.T1 = s + bb;
-    p.Winv = s + 2 * bb;
+    p.Gd = inplace ? const_cast<T*>(e.diag) : e.Gd;
+    p.Gu = inplace ? const_cast<T*>(e.upper) : e.Gu;
+    p.Gl = inplace ? const_cast<T*>(e.lower) : e.Gl;
+    T* sp = reinterpret_cast<T*>(slot);
+    p.T0 = sp;
+    p.T1 = sp + bb;
+    p.T2 = sp + 2 * bb;
+    p.T3 = sp + 3 * bb;
+    p.Winv = sp + 4 * bb;
     T* xp = p.Winv + invert_side_elems(e.b);
-    p.X = save ? e.Gl : xp;
-    p.P = save ? e.Gu : xp + (size_t)(e.n - 1) * bb;
+    p.X = save ? p.Gl : xp;
+    p.P = save ? p.Gu : xp + (size_t)(e.n - 1) * bb;
     p.hdr = hdr;
-    p.status = &inst_status;
+    p.status = &item->status;
     p.n = e.n;
     p.b = e.b;
     p.flags = flags;
+    p.ckpt = nullptr;
+    p.ckpt_every = 1;
     if (e.b <= 32)
       rgf_sweep<T, 32, 32>(team, p, smem);
     else
       rgf_sweep<T, 64, 64>(team, p, smem);
     __syncthreads();
-    if (threadIdx.x == 0) {
-      if (hdr->inst_status) hdr->inst_status[e.orig] = inst_status;
-      if (inst_status) report(&hdr->status, inst_status);
+    if (rank == 0 && threadIdx.x == 0) {
+      int st = *((volatile int*)&item->status);
+      if (hdr->inst_status) hdr->inst_status[e.orig] = st;
+      if (st) report(&hdr->status, st);
     }
-    __syncthreads();  // `next` / `inst_status` are rewritten by the next dequeue
   }
 }
 
@@ -97,7 +143,7 @@ constexpr size_t kBatchedSmem = sizeof(GjShared<cplx>) > (size_t)gemm_smem_elems
 static size_t elem_bytes(int dtype) { return (dtype == SINVB_C128 || dtype == SINVB_C64) ? 16 : 8; }
 
 struct BatchLayout {
-  size_t desc_offset, slots_offset, slot_bytes, total;
+  size_t desc_offset, items_offset, slots_offset, slot_bytes, total;
   unsigned nslots;
 };
 
@@ -113,13 +159,14 @@ static BatchLayout batch_layout(const sinvb_batch_desc* d, int count, int dtype,
   size_t slot = 0;
   for (int k = 0; k < count; k++) {
     size_t bb = (size_t)d[k].b * d[k].b;
-    size_t s = 2 * bb + invert_side_elems(d[k].b);
+    size_t s = 4 * bb + invert_side_elems(d[k].b);
     if (!save) s += 2 * (size_t)(d[k].n - 1) * bb;
     slot = std::max(slot, s * es);
   }
   L.nslots = batch_slots();
   L.desc_offset = sizeof(WsHeader);
-  L.slots_offset = align_up(L.desc_offset + (size_t)count * sizeof(BatchEntry<cplx>), 256);
+  L.items_offset = align_up(L.desc_offset + (size_t)count * sizeof(BatchEntry<cplx>), 256);
+  L.slots_offset = align_up(L.items_offset + (size_t)count * sizeof(ItemArea), 256);
   L.slot_bytes = align_up(std::max<size_t>(slot, 256), 256);
   L.total = L.slots_offset + (size_t)L.nslots * L.slot_bytes;
   return L;
@@ -133,9 +180,11 @@ static int check_batch(const sinvb_batch_desc* d, int count, unsigned flags, con
   const size_t align = elem_bytes(dtype);
   for (int k = 0; k < count; k++) {
     const sinvb_batch_desc& e = d[k];
-    if (e.n < 1 || e.b < 1 || !e.diag || !e.G_diag) return SINVB_EINVAL;
+    const bool inplace = flags & SINVB_INPLACE;
+    if (e.n < 1 || e.b < 1 || !e.diag || (!inplace && !e.G_diag)) return SINVB_EINVAL;
     if (e.n > 1 && (!e.upper || !e.lower)) return SINVB_EINVAL;
-    if (save && e.n > 1 && (!e.G_upper || !e.G_lower)) return SINVB_EINVAL;
+    if (!inplace && save && e.n > 1 && (!e.G_upper || !e.G_lower)) return SINVB_EINVAL;
+    if (inplace && !save) return SINVB_EINVAL;
     for (const void* q : {e.diag, e.upper, e.lower, (const void*)e.G_diag, (const void*)e.G_upper, (const void*)e.G_lower})
       if (q && (uintptr_t)q % align) return SINVB_EINVAL;
   }
@@ -143,14 +192,28 @@ static int check_batch(const sinvb_batch_desc* d, int count, unsigned flags, con
   return check_device();
 }
 
+// CTAs per instance: enough tiles per CTA to stay busy, few enough barriers.
+static int team_size(int b, unsigned flags) {
+  if (flags & SINVB_FORCE_CTA) return 1;
+  if (b >= 1024) return 8;
+  if (b >= 512) return 4;
+  if (b >= 256) return 2;
+  return 1;
+}
+
 template <class T>
-static int launch_batched(void* ws, cudaStream_t stream) {
+static int launch_batched(void* ws, int count, cudaStream_t stream) {
   auto k = rgf_batched_kernel<T>;
   SINVB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchedSmem));
-  // reset status, barrier and queue; the kernel clears per-instance status itself
+  // reset status, barrier and queue, and every instance's team area
   SINVB_CUDA(cudaMemsetAsync(ws, 0, 16, stream));
-  k<<<batch_slots(), kThreads, kBatchedSmem, stream>>>((unsigned char*)ws);
-  SINVB_CUDA(cudaGetLastError());
+  const size_t items_offset = align_up(sizeof(WsHeader) + (size_t)count * sizeof(BatchEntry<cplx>), 256);
+  SINVB_CUDA(cudaMemsetAsync((unsigned char*)ws + items_offset, 0, (size_t)count * sizeof(ItemArea), stream));
+  unsigned char* w = (unsigned char*)ws;
+  void* args[] = {(void*)&w};
+  // cooperative: every CTA resident, so a team member waiting for the others always gets them
+  SINVB_CUDA(cudaLaunchCooperativeKernel((const void*)k, dim3(batch_slots()), dim3(kThreads), args, kBatchedSmem,
+                                         stream));
   return SINVB_OK;
 }
 
@@ -172,12 +235,19 @@ static int upload_and_run(const sinvb_batch_desc* d, int count, unsigned flags, 
     e.n = d[k].n;
     e.b = d[k].b;
     e.orig = k;
-    e.pad = 0;
+    e.team = team_size(e.b, flags);
+    e.slot_start = 0;
+    e.pad[0] = e.pad[1] = e.pad[2] = 0;
   }
   // largest first (cost ~ b^3 n): long chains start while short ones fill in
   std::stable_sort(entries.begin(), entries.end(), [](const BatchEntry<T>& x, const BatchEntry<T>& y) {
     return (double)x.b * x.b * x.b * x.n > (double)y.b * y.b * y.b * y.n;
   });
+  int total_slots = 0;
+  for (auto& e : entries) {
+    e.slot_start = total_slots;
+    total_slots += e.team;
+  }
   WsHeader h{};
   h.count = count;
   h.flags = flags;
@@ -186,12 +256,30 @@ static int upload_and_run(const sinvb_batch_desc* d, int count, unsigned flags, 
   h.desc_offset = L.desc_offset;
   h.slots_offset = L.slots_offset;
   h.inst_status = status;
+  h.items_offset = L.items_offset;
+  h.total_slots = total_slots;
   unsigned char* w = (unsigned char*)ws;
   SINVB_CUDA(cudaMemcpyAsync(w, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
   SINVB_CUDA(cudaMemcpyAsync(w + L.desc_offset, entries.data(), count * sizeof(BatchEntry<T>),
                              cudaMemcpyHostToDevice, stream));
   // the pageable copies above are staged before they return; the host arrays may go
-  return launch_batched<T>(ws, stream);
+  {
+    std::lock_guard<std::mutex> lock(g_count_mutex);
+    count_table()[ws] = count;
+  }
+  return launch_batched<T>(ws, count, stream);
+}
+
+template <class T>
+static int rerun(void* ws, cudaStream_t stream) {
+  int count = -1;
+  {
+    std::lock_guard<std::mutex> lock(g_count_mutex);
+    auto it = count_table().find(ws);
+    if (it != count_table().end()) count = it->second;
+  }
+  if (count < 1) return SINVB_EINVAL;  // nothing uploaded into this workspace
+  return launch_batched<T>(ws, count, stream);
 }
 
 }  // namespace sinvb
@@ -222,13 +310,13 @@ int sinvb_rgf_batched_d(const sinvb_batch_desc* descs, int count, unsigned flags
 int sinvb_rgf_batched_rerun_z(void* workspace, sinvb_stream_t stream) {
   if (!workspace || (uintptr_t)workspace % 256) return SINVB_EINVAL;
   int rc = check_device();
-  return rc ? rc : launch_batched<cplx>(workspace, (cudaStream_t)stream);
+  return rc ? rc : rerun<cplx>(workspace, (cudaStream_t)stream);
 }
 
 int sinvb_rgf_batched_rerun_d(void* workspace, sinvb_stream_t stream) {
   if (!workspace || (uintptr_t)workspace % 256) return SINVB_EINVAL;
   int rc = check_device();
-  return rc ? rc : launch_batched<double>(workspace, (cudaStream_t)stream);
+  return rc ? rc : rerun<double>(workspace, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -1,0 +1,443 @@
+// Block cyclic reduction (BCR) selected inversion on the whole GPU.
+//
+// Reference: src/sinv/algorithms/bcr/bcr_serial.py:19-467 with the padding and
+// production index sets of src/sinv/algorithms/bcr/bcr_utils.py:17-129.
+//
+// The reference pads the block count to 2^p - 1 with identity blocks
+// (bcr_utils.py:44-71) and works on dense N x N arrays.  Padding rows are
+// decoupled from the real rows (zero couplings), so every product they enter is
+// an exact zero and every real block comes out the same without them: this
+// implementation skips them and keeps only block arrays.  It also keeps
+// inv(A_kk) from the reduction instead of recomputing it in the production
+// (bcr_serial.py:302, :379); both computations are the same inversion of the
+// same block.
+//
+// Level l (offset o = 2^l) of the reduction eliminates the rows e = o-1 (mod 2o)
+// into the kept rows j = 2o-1 (mod 2o); the rows of a level are independent
+// (bcr_serial.py:207-212), and so are the produced rows of a production level
+// (bcr_serial.py:437-466).  The host turns the whole algorithm into phases of
+// independent block operations (executor.cuh) that one cooperative kernel
+// runs on every SM:
+//
+//   reduce l:   Dinv[e] = D[e]^{-1}                                   (:121, :148)
+//               U_{e,e+o} = Dinv[e] A_{e,e+o},  L_{e+o,e} = A_{e+o,e} Dinv[e]
+//               U_{e,e-o} = Dinv[e] A_{e,e-o},  L_{e-o,e} = A_{e-o,e} Dinv[e]  (:124-128, :150-154)
+//               D[j] -= L_{j,i} A_{i,j} + L_{j,k} A_{k,j}             (:130-133, :156-159)
+//               A_{j,j-2o} = -L_{j,i} A_{i,j-2o},  A_{j,j+2o} = -L_{j,k} A_{k,j+2o}   (:138-142, :164-168)
+//   root:       G_rr = D[r]^{-1}                                      (:220-249)
+//   produce l:  corner / center production                            (:253-383)
+//
+// Level couplings A_{r,r+o} / A_{r+o,r} (l >= 1) and produced couplings
+// G_{r,r+o} / G_{r+o,r} (l >= 1) live in per-level workspace arrays indexed by
+// q = (r+1)/o - 1; level 0 couplings are the input and output block arrays.
+#include <vector>
+
+#include "executor.cuh"
+#include "host_util.h"
+
+namespace sinvb {
+
+namespace {
+
+// Host-side builder of an executor schedule.
+struct Sched {
+  std::vector<ExecOp> ops;
+  std::vector<ExecPhase> phases;
+  int bm, bn;
+  int cur_units = 0;
+
+  void begin() {
+    ExecPhase p{};
+    p.op_begin = p.op_end = (int)ops.size();
+    phases.push_back(p);
+    cur_units = 0;
+  }
+  void push(ExecOp o) {
+    o.unit_start = cur_units;
+    int u = exec_units(o, bm, bn);
+    if (u == 0) return;
+    cur_units += u;
+    ops.push_back(o);
+    phases.back().op_end = (int)ops.size();
+    phases.back().units = cur_units;
+  }
+  // C = D + alpha (A B [+ A2 B2]); all blocks m x m with leading dimension ld.
+  void gemm(int m, double alpha, const void* A, const void* B, const void* D, void* C, const void* A2 = nullptr,
+            const void* B2 = nullptr, int ld = -1, int M = -1, int N = -1, int K = -1, int lda = -1, int ldb = -1,
+            int ldc = -1, int ldd = -1) {
+    ExecOp o{};
+    o.kind = kExecGemm;
+    o.M = M < 0 ? m : M;
+    o.N = N < 0 ? m : N;
+    o.K = K < 0 ? m : K;
+    int l = ld < 0 ? m : ld;
+    o.lda = lda < 0 ? l : lda;
+    o.ldb = ldb < 0 ? l : ldb;
+    o.ldc = ldc < 0 ? l : ldc;
+    o.ldd = ldd < 0 ? l : ldd;
+    o.alpha = alpha;
+    o.A = A; o.B = B; o.D = D; o.C = C;
+    if (A2) {
+      o.A2 = A2; o.B2 = B2;
+      o.K2 = o.K; o.lda2 = o.lda; o.ldb2 = o.ldb;
+    }
+    push(o);
+  }
+  void gj(int m, void* blk, int ld) {
+    ExecOp o{};
+    o.kind = kExecGj;
+    o.M = m;
+    o.ldc = ld;
+    o.C = blk;
+    push(o);
+  }
+  void copy(int rows, int cols, const void* src, int lds, void* dst, int ldd, bool transpose = false) {
+    ExecOp o{};
+    o.kind = kExecCopy;
+    o.M = rows;
+    o.N = cols;
+    o.lda = lds;
+    o.ldc = ldd;
+    o.transpose = transpose;
+    o.A = src;
+    o.C = dst;
+    push(o);
+  }
+};
+
+// Phases of a blocked Gauss-Jordan inversion (the schedule form of
+// team_invert) of every m x m block in blks; side[x] holds the W / R panels of
+// block x (invert_side_elems(m) elements).
+template <class T>
+void invert_many(Sched& s, const std::vector<T*>& blks, const std::vector<T*>& side, int m) {
+  if (blks.empty()) return;
+  if (m <= kGjMax) {
+    s.begin();
+    for (T* a : blks) s.gj(m, a, m);
+    return;
+  }
+  const int np = (m + kPanel - 1) / kPanel;
+  int pK0 = -1, pkb = 0;
+  auto W = [&](size_t x) { return side[x]; };
+  auto R = [&](size_t x) { return side[x] + (size_t)m * kPanel; };
+  auto write_back = [&](size_t x) {
+    T* a = blks[x];
+    const int r1 = pK0 + pkb;
+    s.copy(pK0, pkb, W(x), kPanel, a + pK0, m);
+    s.copy(m - r1, pkb, W(x) + (size_t)r1 * kPanel, kPanel, a + (size_t)r1 * m + pK0, m);
+    s.copy(pkb, pK0, R(x), m, a + (size_t)pK0 * m, m);
+    s.copy(pkb, m - r1, R(x) + r1, m, a + (size_t)pK0 * m + r1, m);
+  };
+  for (int p = 0; p < np; p++) {
+    const int K0 = p * kPanel, kb = std::min(kPanel, m - K0), right = K0 + kb;
+    s.begin();
+    for (size_t x = 0; x < blks.size(); x++) {
+      s.gj(kb, blks[x] + (size_t)K0 * m + K0, m);
+      if (pK0 >= 0) write_back(x);
+    }
+    s.begin();
+    for (size_t x = 0; x < blks.size(); x++) {
+      T* a = blks[x];
+      T* Dinv = a + (size_t)K0 * m + K0;
+      T* row = a + (size_t)K0 * m;
+      s.gemm(m, 1.0, Dinv, row, nullptr, R(x), nullptr, nullptr, m, kb, K0, kb);
+      s.gemm(m, 1.0, Dinv, row + right, nullptr, R(x) + right, nullptr, nullptr, m, kb, m - right, kb);
+    }
+    s.begin();
+    for (size_t x = 0; x < blks.size(); x++) {
+      T* a = blks[x];
+      T* Dinv = a + (size_t)K0 * m + K0;
+      int rs[2] = {0, right}, rn[2] = {K0, m - right};
+      for (int ri = 0; ri < 2; ri++) {
+        T* colK = a + (size_t)rs[ri] * m + K0;
+        for (int ci = 0; ci < 2; ci++) {
+          T* C = a + (size_t)rs[ri] * m + rs[ci];
+          s.gemm(m, -1.0, colK, R(x) + rs[ci], C, C, nullptr, nullptr, m, rn[ri], rn[ci], kb);
+        }
+        s.gemm(m, -1.0, colK, Dinv, nullptr, W(x) + (size_t)rs[ri] * kPanel, nullptr, nullptr, m, rn[ri], kb, kb,
+               m, m, kPanel);
+      }
+    }
+    pK0 = K0;
+    pkb = kb;
+  }
+  s.begin();
+  for (size_t x = 0; x < blks.size(); x++) write_back(x);
+}
+
+struct BcrPlan {
+  // data offsets in elements from the data base
+  size_t D, Dinv, Ua, Ub, La, Lb, W;
+  std::vector<size_t> Up, Lo, CU, CL;  // per level (index 0 unused)
+  size_t data_elems;
+  int height, root;
+};
+
+inline int ceil_log2(long long x) {
+  int p = 0;
+  while ((1LL << p) < x) p++;
+  return p;
+}
+
+BcrPlan bcr_plan(int n, int b) {
+  BcrPlan P{};
+  const size_t bb = (size_t)b * b;
+  const int p = ceil_log2((long long)n + 1);  // padded count 2^p - 1 (bcr_utils.py:17-40)
+  P.height = p - 1;
+  P.root = (1 << (p - 1)) - 1;
+  size_t off = 0;
+  auto take = [&](size_t blocks) {
+    size_t at = off;
+    off += blocks * bb;
+    return at;
+  };
+  P.D = take(n);
+  P.Dinv = take(n);
+  P.Ua = take(n);
+  P.Ub = take(n);
+  P.La = take(n);
+  P.Lb = take(n);
+  P.Up.assign(P.height + 2, 0);
+  P.Lo.assign(P.height + 2, 0);
+  P.CU.assign(P.height + 2, 0);
+  P.CL.assign(P.height + 2, 0);
+  for (int l = 1; l <= P.height; l++) {
+    size_t cnt = (size_t)(n >> l);
+    P.Up[l] = take(cnt);
+    P.Lo[l] = take(cnt);
+    P.CU[l] = take(cnt);
+    P.CL[l] = take(cnt);
+  }
+  P.W = off;
+  off += (size_t)(n / 2 + 2) * invert_side_elems(b);
+  P.data_elems = off;
+  return P;
+}
+
+template <class T>
+void build_bcr(Sched& s, const BcrPlan& P, int n, int b, const T* diag, const T* upper, const T* lower, T* Gd, T* Gu,
+               T* Gl, T* base) {
+  const size_t bb = (size_t)b * b;
+  auto blk = [&](size_t region, int r) { return base + region + (size_t)r * bb; };
+  T* D = base + P.D;
+  auto Dk = [&](int r) { return D + (size_t)r * bb; };
+  auto Dinv = [&](int r) { return blk(P.Dinv, r); };
+  auto Ua = [&](int r) { return blk(P.Ua, r); };
+  auto Ub = [&](int r) { return blk(P.Ub, r); };
+  auto La = [&](int r) { return blk(P.La, r); };
+  auto Lb = [&](int r) { return blk(P.Lb, r); };
+  auto q = [](int r, int l) { return (r + 1) / (1 << l) - 1; };
+  // level-l couplings of the reduced matrix: A_{r,r+o}, A_{r+o,r}
+  auto Up = [&](int l, int r) -> T* { return l == 0 ? const_cast<T*>(upper) + (size_t)r * bb : blk(P.Up[l], q(r, l)); };
+  auto Lo = [&](int l, int r) -> T* { return l == 0 ? const_cast<T*>(lower) + (size_t)r * bb : blk(P.Lo[l], q(r, l)); };
+  // produced couplings G_{r,r+o}, G_{r+o,r}
+  auto CU = [&](int l, int r) -> T* { return l == 0 ? Gu + (size_t)r * bb : blk(P.CU[l], q(r, l)); };
+  auto CL = [&](int l, int r) -> T* { return l == 0 ? Gl + (size_t)r * bb : blk(P.CL[l], q(r, l)); };
+  std::vector<T*> Wv;
+  for (int x = 0; x < n / 2 + 2; x++) Wv.push_back(base + P.W + (size_t)x * invert_side_elems(b));
+
+  s.begin();
+  s.copy(n * b, b, diag, b, D, b);  // working diagonal (the reference reduces a copy, bcr_utils.py:66-69)
+  for (int l = 0; l < P.height; l++) {
+    const int o = 1 << l;
+    std::vector<int> E;
+    for (int e = o - 1; e < n; e += 2 * o) E.push_back(e);
+    // Dinv[e] = D[e]^{-1}
+    s.begin();
+    std::vector<T*> inv;
+    for (int e : E) {
+      s.copy(b, b, Dk(e), b, Dinv(e), b);
+      inv.push_back(Dinv(e));
+    }
+    invert_many<T>(s, inv, Wv, b);
+    // U / L factors of every eliminated row
+    s.begin();
+    for (int e : E) {
+      const int a = e - o, c = e + o;
+      if (c <= n - 1) {
+        s.gemm(b, 1.0, Dinv(e), Up(l, e), nullptr, Ub(e));
+        s.gemm(b, 1.0, Lo(l, e), Dinv(e), nullptr, Lb(e));
+      }
+      if (a >= 0) {
+        s.gemm(b, 1.0, Dinv(e), Lo(l, a), nullptr, Ua(e));
+        s.gemm(b, 1.0, Up(l, a), Dinv(e), nullptr, La(e));
+      }
+    }
+    // Schur update of the kept rows and the next level's couplings
+    s.begin();
+    for (int j = 2 * o - 1; j < n; j += 2 * o) {
+      const int i = j - o, k = j + o;
+      if (k <= n - 1)
+        s.gemm(b, -1.0, Lb(i), Up(l, i), Dk(j), Dk(j), La(k), Lo(l, j));
+      else
+        s.gemm(b, -1.0, Lb(i), Up(l, i), Dk(j), Dk(j));
+      const int h = j - 2 * o, r = k + o;
+      if (h >= 0) s.gemm(b, -1.0, Lb(i), Lo(l, h), nullptr, Lo(l + 1, h));
+      if (r <= n - 1) s.gemm(b, -1.0, La(k), Up(l, k), nullptr, Up(l + 1, j));
+    }
+  }
+  // root
+  s.begin();
+  s.copy(b, b, Dk(P.root), b, Gd + (size_t)P.root * bb, b);
+  invert_many<T>(s, std::vector<T*>{Gd + (size_t)P.root * bb}, Wv, b);
+  // production, top level down
+  for (int l = P.height - 1; l >= 0; l--) {
+    const int o = 1 << l;
+    std::vector<int> E;
+    for (int e = o - 1; e < n; e += 2 * o) E.push_back(e);
+    s.begin();
+    for (int e : E) {
+      const int a = e - o, c = e + o;
+      const bool ha = a >= 0, hc = c <= n - 1;
+      T* Gaa = ha ? Gd + (size_t)a * bb : nullptr;
+      T* Gcc = hc ? Gd + (size_t)c * bb : nullptr;
+      if (ha && hc) {  // center_produce, bcr_serial.py:361-383
+        T* Gac = CU(l + 1, a);
+        T* Gca = CL(l + 1, a);
+        s.gemm(b, -1.0, Gaa, La(e), nullptr, CU(l, a), Gac, Lb(e));
+        s.gemm(b, -1.0, Gca, La(e), nullptr, CL(l, e), Gcc, Lb(e));
+        s.gemm(b, -1.0, Ua(e), Gaa, nullptr, CL(l, a), Ub(e), Gca);
+        s.gemm(b, -1.0, Ua(e), Gac, nullptr, CU(l, e), Ub(e), Gcc);
+      } else if (hc) {  // corner_produce from below, bcr_serial.py:291-298
+        s.gemm(b, -1.0, Gcc, Lb(e), nullptr, CL(l, e));
+        s.gemm(b, -1.0, Ub(e), Gcc, nullptr, CU(l, e));
+      } else if (ha) {  // corner_produce from above
+        s.gemm(b, -1.0, Gaa, La(e), nullptr, CU(l, a));
+        s.gemm(b, -1.0, Ua(e), Gaa, nullptr, CL(l, a));
+      }
+    }
+    s.begin();
+    for (int e : E) {
+      const int a = e - o, c = e + o;
+      const bool ha = a >= 0, hc = c <= n - 1;
+      T* Gee = Gd + (size_t)e * bb;
+      if (ha && hc)
+        s.gemm(b, -1.0, CL(l, a), La(e), Dinv(e), Gee, CU(l, e), Lb(e));
+      else if (hc)
+        s.gemm(b, -1.0, CU(l, e), Lb(e), Dinv(e), Gee);
+      else if (ha)
+        s.gemm(b, -1.0, CL(l, a), La(e), Dinv(e), Gee);
+    }
+  }
+  // drop empty phases
+  std::vector<ExecPhase> kept;
+  for (auto& p : s.phases)
+    if (p.units > 0) kept.push_back(p);
+  s.phases.swap(kept);
+}
+
+struct BcrLayout {
+  size_t ops_off, phases_off, data_off, total;
+  int nops, nphases;
+};
+
+int tile_for(int b) { return b >= 128 ? 64 : 32; }
+
+template <class T>
+BcrLayout bcr_layout_and_schedule(int n, int b, const T* diag, const T* upper, const T* lower, T* Gd, T* Gu, T* Gl,
+                                  unsigned char* ws, Sched* out) {
+  const BcrPlan P = bcr_plan(n, b);
+  BcrLayout L{};
+  Sched s;
+  s.bm = s.bn = tile_for(b);
+  // the op table size does not depend on the pointers: build once to size it
+  L.ops_off = sizeof(WsHeader);
+  build_bcr<T>(s, P, n, b, diag, upper, lower, Gd, Gu, Gl, (T*)nullptr);
+  L.nops = (int)s.ops.size();
+  L.nphases = (int)s.phases.size();
+  L.phases_off = align_up(L.ops_off + (size_t)L.nops * sizeof(ExecOp), 256);
+  L.data_off = align_up(L.phases_off + (size_t)L.nphases * sizeof(ExecPhase), 256);
+  L.total = align_up(L.data_off + P.data_elems * sizeof(T), 256);
+  if (out && ws) {
+    out->bm = out->bn = s.bm;
+    build_bcr<T>(*out, P, n, b, diag, upper, lower, Gd, Gu, Gl, (T*)(ws + L.data_off));
+  }
+  return L;
+}
+
+template <class T, int BM, int BN>
+__global__ void __launch_bounds__(kThreads, 1) bcr_kernel(unsigned char* ws, int nphases) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
+  const ExecOp* ops = reinterpret_cast<const ExecOp*>(ws + hdr->desc_offset);
+  const ExecPhase* phases = reinterpret_cast<const ExecPhase*>(ws + hdr->items_offset);
+  TeamDyn team{&hdr->barrier_count, &hdr->status, (int)blockIdx.x, (int)gridDim.x, 0u};
+  run_schedule<T, BM, BN>(team, ops, phases, nphases, &hdr->status, reinterpret_cast<T*>(smem_raw));
+}
+
+template <class T, int BM, int BN>
+int launch_bcr(unsigned char* ws, int nphases, cudaStream_t stream) {
+  constexpr size_t g = (size_t)gemm_smem_elems<T, BM, BN>() * sizeof(T);
+  constexpr size_t smem = g > sizeof(GjShared<T>) ? g : sizeof(GjShared<T>);
+  auto k = bcr_kernel<T, BM, BN>;
+  SINVB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  void* args[] = {(void*)&ws, (void*)&nphases};
+  SINVB_CUDA(cudaLaunchCooperativeKernel((const void*)k, dim3(device_sm_count()), dim3(kThreads), args, smem,
+                                         stream));
+  return SINVB_OK;
+}
+
+template <class T>
+int run_bcr(const void* diag, const void* upper, const void* lower, int n, int b, unsigned flags, void* Gd,
+            void* Gu, void* Gl, void* workspace, size_t ws_bytes, cudaStream_t stream, int dtype) {
+  (void)flags;
+  if (n < 1 || b < 1 || !diag || !Gd || !workspace) return SINVB_EINVAL;
+  if (n > 1 && (!upper || !lower || !Gu || !Gl)) return SINVB_EINVAL;
+  if ((uintptr_t)workspace % 256) return SINVB_EWORKSPACE;
+  const size_t align = sizeof(T);
+  for (const void* p : {diag, upper, lower, (const void*)Gd, (const void*)Gu, (const void*)Gl})
+    if (p && (uintptr_t)p % align) return SINVB_EINVAL;
+  int rc = check_device();
+  if (rc) return rc;
+  unsigned char* ws = (unsigned char*)workspace;
+  Sched s;
+  BcrLayout L = bcr_layout_and_schedule<T>(n, b, (const T*)diag, (const T*)upper, (const T*)lower, (T*)Gd, (T*)Gu,
+                                           (T*)Gl, ws, &s);
+  if (ws_bytes < L.total) return SINVB_EWORKSPACE;
+  (void)dtype;
+  WsHeader h{};
+  h.desc_offset = L.ops_off;
+  h.items_offset = L.phases_off;
+  SINVB_CUDA(cudaMemcpyAsync(ws, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
+  SINVB_CUDA(cudaMemcpyAsync(ws + L.ops_off, s.ops.data(), s.ops.size() * sizeof(ExecOp), cudaMemcpyHostToDevice,
+                             stream));
+  SINVB_CUDA(cudaMemcpyAsync(ws + L.phases_off, s.phases.data(), s.phases.size() * sizeof(ExecPhase),
+                             cudaMemcpyHostToDevice, stream));
+  if (tile_for(b) == 64) return launch_bcr<T, 64, 64>(ws, (int)s.phases.size(), stream);
+  return launch_bcr<T, 32, 32>(ws, (int)s.phases.size(), stream);
+}
+
+}  // namespace
+
+}  // namespace sinvb
+
+using namespace sinvb;
+
+extern "C" {
+
+size_t sinvb_bcr_workspace_size(int n, int b, int dtype, unsigned flags) {
+  (void)flags;
+  if (n < 1 || b < 1) return 0;
+  if (dtype == SINVB_C128)
+    return bcr_layout_and_schedule<cplx>(n, b, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr)
+        .total;
+  if (dtype == SINVB_F64)
+    return bcr_layout_and_schedule<double>(n, b, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                           nullptr)
+        .total;
+  return 0;
+}
+
+int sinvb_bcr_z(const void* diag, const void* upper, const void* lower, int n, int b, unsigned flags, void* G_diag,
+                void* G_upper, void* G_lower, void* workspace, size_t workspace_bytes, sinvb_stream_t stream) {
+  return run_bcr<cplx>(diag, upper, lower, n, b, flags, G_diag, G_upper, G_lower, workspace, workspace_bytes,
+                       (cudaStream_t)stream, SINVB_C128);
+}
+
+int sinvb_bcr_d(const void* diag, const void* upper, const void* lower, int n, int b, unsigned flags, void* G_diag,
+                void* G_upper, void* G_lower, void* workspace, size_t workspace_bytes, sinvb_stream_t stream) {
+  return run_bcr<double>(diag, upper, lower, n, b, flags, G_diag, G_upper, G_lower, workspace, workspace_bytes,
+                         (cudaStream_t)stream, SINVB_F64);
+}
+
+}  // extern "C"

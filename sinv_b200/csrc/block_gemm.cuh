@@ -1,43 +1,73 @@
 // Block GEMM on the FP64 tensor cores (DMMA, mma.sync m8n8k4.f64).
 //
-//   C[M x N] = D + alpha * A[M x K] * B[K x N]        (row-major, any sizes)
+//   C[M x N] = beta D + alpha ( op(A) op(B) + sign2 op(A2) op(B2) )
+//
+// op(X) is X or X^H (conjugate transpose; plain transpose for real types),
+// D may alias C (each tile reads its own D before writing), the second product
+// is optional (BCR's productions are two-term sums,
+// src/sinv/algorithms/bcr/bcr_serial.py:361-383; the adjoint sweeps need
+// signed sums of conjugate-transposed products).
 //
 // Complex products run as four real DMMA products (4M):
 //   C.re += A.re B.re - A.im B.im,   C.im += A.re B.im + A.im B.re
-// B200 has no FP64 kind of tcgen05.mma; the warp-level DMMA path peaks at the
-// same 37 TFLOP/s as the chip's FP64 units (measured), one CTA per SM reaching
-// its 0.25 TFLOP/s share with 8 warps.
+// with conjugation and the sign of the second product applied to the register
+// fragments.  B200 has no FP64 kind of tcgen05.mma; the warp-level DMMA path
+// peaks at the chip's FP64 rate (37 TFLOP/s measured), one CTA of 8 warps per SM
+// reaching its 0.25 TFLOP/s share.
 //
 // A CTA computes one BM x BN output tile.  K is streamed through shared memory
-// in BK-element chunks with a 3-stage cp.async ring.  Shared-memory layouts are
-// XOR-swizzled so the DMMA fragment loads (A[g][t] and B[t][g], lane = 4g + t)
-// hit distinct banks:
+// in BK-element chunks with a 3-stage cp.async ring; the first product's K is
+// padded with zeros to a chunk boundary so a chunk never mixes products.
+// Shared-memory layouts are XOR-swizzled so the DMMA fragment loads
+// (A[g][t] and B[t][g], lane = 4g + t) hit distinct banks:
 //   complex (16 B):  A(m,k) -> m*BK + (k ^ ((m&1)<<2)),  B(k,n) -> k*BN + (n ^ ((k&3)<<1))
 //   real    ( 8 B):  A(m,k) -> m*BK + (k ^ ((m&3)<<2)),  B(k,n) -> k*BN + (n ^ ((k&3)<<2))
+// Global loads are coalesced for either operand form (the fastest-varying
+// thread index follows the contiguous source dimension).
 #pragma once
 
 #include "common.cuh"
 
 namespace sinvb {
 
+enum : int { kOpN = 0, kOpH = 1 };
+
 template <class T>
 struct GemmOp {
   const T* A;
   const T* B;
-  const T* D;  // addend, may be null, may alias C (read before the tile's own write)
+  const T* D;  // addend, may be null, may alias C
   T* C;
   int lda, ldb, ldd, ldc;
   int M, N, K;
-  double alpha;
+  double alpha, beta;
+  int opA, opB;
+  const T* A2;  // second product (null: none); op(A2) is M x K2, op(B2) is K2 x N
+  const T* B2;
+  int lda2, ldb2, K2;
+  int opA2, opB2;
+  int sign2;  // +1 or -1
 };
 
 template <class T>
-__device__ __forceinline__ GemmOp<T> make_op(int M, int N, int K, double alpha, const T* A, int lda,
-                                             const T* B, int ldb, const T* D, int ldd, T* C, int ldc) {
+__host__ __device__ __forceinline__ GemmOp<T> make_op(int M, int N, int K, double alpha, const T* A, int lda,
+                                                      const T* B, int ldb, const T* D, int ldd, T* C, int ldc) {
   GemmOp<T> o;
   o.A = A; o.B = B; o.D = D; o.C = C;
   o.lda = lda; o.ldb = ldb; o.ldd = ldd; o.ldc = ldc;
-  o.M = M; o.N = N; o.K = K; o.alpha = alpha;
+  o.M = M; o.N = N; o.K = K; o.alpha = alpha; o.beta = 1.0;
+  o.opA = kOpN; o.opB = kOpN;
+  o.A2 = nullptr; o.B2 = nullptr; o.lda2 = 0; o.ldb2 = 0; o.K2 = 0;
+  o.opA2 = kOpN; o.opB2 = kOpN; o.sign2 = 1;
+  return o;
+}
+
+// Adds the second product sign2 * op(A2) op(B2) (K2 = K) to an op.
+template <class T>
+__host__ __device__ __forceinline__ GemmOp<T> with_second(GemmOp<T> o, const T* A2, int lda2, int opA2, const T* B2,
+                                                          int ldb2, int opB2, int sign2 = 1) {
+  o.A2 = A2; o.B2 = B2; o.lda2 = lda2; o.ldb2 = ldb2; o.K2 = o.K;
+  o.opA2 = opA2; o.opB2 = opB2; o.sign2 = sign2;
   return o;
 }
 
@@ -58,28 +88,48 @@ template <> struct GemmCfg<double> {
 
 // Shared memory (in elements of T) one CTA tile needs.
 template <class T, int BM, int BN>
-constexpr int gemm_smem_elems() {
+__host__ __device__ constexpr int gemm_smem_elems() {
   return kStages * (BM * GemmCfg<T>::BK + GemmCfg<T>::BK * BN);
+}
+
+// K extent of the first product as streamed: padded to whole chunks when a
+// second product follows.
+template <class T>
+__device__ __forceinline__ int k1_padded(const GemmOp<T>& op) {
+  constexpr int BK = GemmCfg<T>::BK;
+  return op.K2 > 0 ? (op.K + BK - 1) / BK * BK : op.K;
 }
 
 template <class T, int BM, int BN>
 __device__ __forceinline__ void load_chunk(const GemmOp<T>& op, int row0, int col0, int k0, T* sA, T* sB) {
   constexpr int BK = GemmCfg<T>::BK;
   const int tid = threadIdx.x;
+  const int K1p = k1_padded(op);
+  const bool second = op.K2 > 0 && k0 >= K1p;
+  const T* A = second ? op.A2 : op.A;
+  const T* B = second ? op.B2 : op.B;
+  const int lda = second ? op.lda2 : op.lda, ldb = second ? op.ldb2 : op.ldb;
+  const int opA = second ? op.opA2 : op.opA, opB = second ? op.opB2 : op.opB;
+  const int kbase = second ? k0 - K1p : k0;
+  const int Klim = second ? op.K2 : op.K;
 #pragma unroll
   for (int e = tid; e < BM * BK; e += kThreads) {
-    int m = e / BK, k = e % BK;
-    int gr = row0 + m, gk = k0 + k;
-    bool v = gr < op.M && gk < op.K;
-    const T* src = v ? op.A + (size_t)gr * op.lda + gk : op.A;
+    int m, k;
+    if (opA == kOpN) { m = e / BK; k = e % BK; } else { k = e / BM; m = e % BM; }
+    const int gr = row0 + m, gk = kbase + k;
+    const bool v = gr < op.M && gk < Klim;
+    const T* src = A;
+    if (v) src = opA == kOpN ? A + (size_t)gr * lda + gk : A + (size_t)gk * lda + gr;
     cp_async_elem<T>(sA + GemmCfg<T>::a_idx(m, k), src, v);
   }
 #pragma unroll
   for (int e = tid; e < BK * BN; e += kThreads) {
-    int k = e / BN, n = e % BN;
-    int gk = k0 + k, gc = col0 + n;
-    bool v = gk < op.K && gc < op.N;
-    const T* src = v ? op.B + (size_t)gk * op.ldb + gc : op.B;
+    int k, n;
+    if (opB == kOpN) { k = e / BN; n = e % BN; } else { n = e / BK; k = e % BK; }
+    const int gk = kbase + k, gc = col0 + n;
+    const bool v = gk < Klim && gc < op.N;
+    const T* src = B;
+    if (v) src = opB == kOpN ? B + (size_t)gk * ldb + gc : B + (size_t)gc * ldb + gk;
     cp_async_elem<T>(sB + GemmCfg<T>::template b_idx<BN>(k, n), src, v);
   }
 }
@@ -92,8 +142,11 @@ struct WarpShape {
   static_assert(MT >= 1 && NT >= 1, "tile too small for 8 warps");
 };
 
+// Fragment signs of a chunk: A.im *= sai (conjugation), B.re *= sbr, B.im *= sbi
+// (conjugation and the sign of the second product).
 template <int BM, int BN>
-__device__ __forceinline__ void mma_chunk(const cplx* sA, const cplx* sB, double (&acc)[WarpShape<BM, BN>::MT][WarpShape<BM, BN>::NT][4]) {
+__device__ __forceinline__ void mma_chunk(const cplx* sA, const cplx* sB, double (&acc)[WarpShape<BM, BN>::MT][WarpShape<BM, BN>::NT][4],
+                                          double sai, double sbr, double sbi) {
   using W = WarpShape<BM, BN>;
   constexpr int BK = GemmCfg<cplx>::BK;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -103,9 +156,16 @@ __device__ __forceinline__ void mma_chunk(const cplx* sA, const cplx* sB, double
   for (int kk = 0; kk < BK; kk += 4) {
     cplx a[W::MT], b[W::NT];
 #pragma unroll
-    for (int mt = 0; mt < W::MT; mt++) a[mt] = sA[GemmCfg<cplx>::a_idx(wm + mt * 8 + g, kk + t)];
+    for (int mt = 0; mt < W::MT; mt++) {
+      a[mt] = sA[GemmCfg<cplx>::a_idx(wm + mt * 8 + g, kk + t)];
+      a[mt].im *= sai;
+    }
 #pragma unroll
-    for (int nt = 0; nt < W::NT; nt++) b[nt] = sB[GemmCfg<cplx>::b_idx<BN>(kk + t, wn + nt * 8 + g)];
+    for (int nt = 0; nt < W::NT; nt++) {
+      b[nt] = sB[GemmCfg<cplx>::b_idx<BN>(kk + t, wn + nt * 8 + g)];
+      b[nt].re *= sbr;
+      b[nt].im *= sbi;
+    }
 #pragma unroll
     for (int mt = 0; mt < W::MT; mt++)
 #pragma unroll
@@ -119,7 +179,8 @@ __device__ __forceinline__ void mma_chunk(const cplx* sA, const cplx* sB, double
 }
 
 template <int BM, int BN>
-__device__ __forceinline__ void mma_chunk(const double* sA, const double* sB, double (&acc)[WarpShape<BM, BN>::MT][WarpShape<BM, BN>::NT][4]) {
+__device__ __forceinline__ void mma_chunk(const double* sA, const double* sB, double (&acc)[WarpShape<BM, BN>::MT][WarpShape<BM, BN>::NT][4],
+                                          double, double sbr, double) {
   using W = WarpShape<BM, BN>;
   constexpr int BK = GemmCfg<double>::BK;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -131,7 +192,7 @@ __device__ __forceinline__ void mma_chunk(const double* sA, const double* sB, do
 #pragma unroll
     for (int mt = 0; mt < W::MT; mt++) a[mt] = sA[GemmCfg<double>::a_idx(wm + mt * 8 + g, kk + t)];
 #pragma unroll
-    for (int nt = 0; nt < W::NT; nt++) b[nt] = sB[GemmCfg<double>::b_idx<BN>(kk + t, wn + nt * 8 + g)];
+    for (int nt = 0; nt < W::NT; nt++) b[nt] = sbr * sB[GemmCfg<double>::b_idx<BN>(kk + t, wn + nt * 8 + g)];
 #pragma unroll
     for (int mt = 0; mt < W::MT; mt++)
 #pragma unroll
@@ -145,13 +206,16 @@ __device__ __forceinline__ void store_pair(const GemmOp<T>& op, int r, int c, do
 template <>
 __device__ __forceinline__ void store_pair<cplx>(const GemmOp<cplx>& op, int r, int c, double v0r, double v0i, double v1r, double v1i) {
   if (r >= op.M) return;
-  const double al = op.alpha;
+  const double al = op.alpha, be = op.beta;
 #pragma unroll
   for (int j = 0; j < 2; j++) {
     int cc = c + j;
     if (cc < op.N) {
       cplx v = j == 0 ? cplx{al * v0r, al * v0i} : cplx{al * v1r, al * v1i};
-      if (op.D) v = op.D[(size_t)r * op.ldd + cc] + v;
+      if (op.D) {
+        cplx d = op.D[(size_t)r * op.ldd + cc];
+        v = be == 1.0 ? d + v : cplx{fma(be, d.re, v.re), fma(be, d.im, v.im)};
+      }
       op.C[(size_t)r * op.ldc + cc] = v;
     }
   }
@@ -159,15 +223,15 @@ __device__ __forceinline__ void store_pair<cplx>(const GemmOp<cplx>& op, int r, 
 template <>
 __device__ __forceinline__ void store_pair<double>(const GemmOp<double>& op, int r, int c, double v0, double, double v1, double) {
   if (r >= op.M) return;
-  const double al = op.alpha;
+  const double al = op.alpha, be = op.beta;
   if (c < op.N) {
     double v = al * v0;
-    if (op.D) v += op.D[(size_t)r * op.ldd + c];
+    if (op.D) v = fma(be, op.D[(size_t)r * op.ldd + c], v);
     op.C[(size_t)r * op.ldc + c] = v;
   }
   if (c + 1 < op.N) {
     double v = al * v1;
-    if (op.D) v += op.D[(size_t)r * op.ldd + c + 1];
+    if (op.D) v = fma(be, op.D[(size_t)r * op.ldd + c + 1], v);
     op.C[(size_t)r * op.ldc + c + 1] = v;
   }
 }
@@ -190,7 +254,13 @@ __device__ void cta_gemm_tile(const GemmOp<T>& op, int tm, int tn, T* smem) {
 #pragma unroll
       for (int q = 0; q < 4; q++) acc[i][j][q] = 0.0;
 
-  const int nk = (op.K + BK - 1) / BK;
+  const int K1p = k1_padded(op);
+  const int nk = (K1p + op.K2 + BK - 1) / BK;
+  const int nk1 = (K1p + BK - 1) / BK;  // chunks of the first product
+  // fragment signs per product: conjugation of A / B, sign of the second product
+  const double sai1 = op.opA == kOpH ? -1.0 : 1.0, sbi1 = op.opB == kOpH ? -1.0 : 1.0;
+  const double s2 = op.sign2 < 0 ? -1.0 : 1.0;
+  const double sai2 = op.opA2 == kOpH ? -1.0 : 1.0, sbi2 = (op.opB2 == kOpH ? -1.0 : 1.0) * s2;
 #pragma unroll
   for (int s = 0; s < kStages - 1; s++) {
     if (s < nk) load_chunk<T, BM, BN>(op, row0, col0, s * BK, sA + s * BM * BK, sB + s * BK * BN);
@@ -206,7 +276,10 @@ __device__ void cta_gemm_tile(const GemmOp<T>& op, int tm, int tn, T* smem) {
     }
     cp_async_commit();
     int st = kc % kStages;
-    mma_chunk<BM, BN>(sA + st * BM * BK, sB + st * BK * BN, acc);
+    if (kc < nk1)
+      mma_chunk<BM, BN>(sA + st * BM * BK, sB + st * BK * BN, acc, sai1, 1.0, sbi1);
+    else
+      mma_chunk<BM, BN>(sA + st * BM * BK, sB + st * BK * BN, acc, sai2, s2, sbi2);
   }
   cp_async_wait<0>();
 

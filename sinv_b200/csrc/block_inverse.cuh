@@ -14,28 +14,36 @@
 //   (ty, tx) of a 16 x 16 grid owns rows ty+16r and columns tx+16c); row k,
 //   column k and 1/a_kk are published through double-buffered shared arrays,
 //   so one barrier per step suffices.
-// * team_invert: any m.  Blocked Gauss-Jordan over 64-wide panels:
+// * team_invert: any m.  Blocked Gauss-Jordan over 32-wide panels:
 //   (1) invert the diagonal panel block with cta_gj_invert,
-//   (2) scale the row panel by it (DMMA GEMM, in place),
-//   (3) rank-64 update of every other block and the new column panel
-//       (DMMA GEMMs), the column panel going to a side buffer that is copied
-//       back while the next pivot block is inverted.
+//   (2) scale the row panel by it (DMMA GEMM) into a side buffer,
+//   (3) rank-32 update of every other block and the new column panel
+//       (DMMA GEMMs), the column panel going to a side buffer; both panels
+//       are copied back while the next pivot block is inverted.
 #pragma once
 
 #include "block_gemm.cuh"
 
 namespace sinvb {
 
-constexpr int kPanel = 64;
+// Blocks of at most kGjMax rows are inverted unblocked by one CTA.  Larger
+// blocks go in panels: the explicit inverse of each pivot block costs accuracy
+// on blocks far from diagonal dominance.  RGF inverts the damped Schur
+// complements S_i and keeps 64-wide panels (tight-binding: ~1e-12 vs 2e-13
+// unblocked); BCR inverts raw reduced diagonal blocks, where 64-wide panels
+// lost three digits (1.8e-9 vs 3e-12) and 32-wide panels lose about one.
+constexpr int kGjMax = 64;
+constexpr int kPanelRgf = 64;
+constexpr int kPanel = 32;  // BCR
 
 template <class T>
 struct GjShared {
-  T rowbuf[2][kPanel];
-  T colbuf[2][kPanel];
+  T rowbuf[2][kGjMax];
+  T colbuf[2][kGjMax];
   T pinv[2];
 };
 
-// Inverts the m x m block at a (leading dimension lda), m <= 64, in place.
+// Inverts the m x m block at a (leading dimension lda), m <= kGjMax, in place.
 // Returns false (and reports) on a zero / non-finite pivot; the block then
 // holds non-finite values.
 template <class T>
@@ -129,69 +137,73 @@ __device__ void team_copy(Team& team, int rows, int cols, const T* src, int lds,
   }
 }
 
-// Bytes of side buffer team_invert needs for an m x m block.
-__host__ __device__ inline size_t invert_side_elems(int m) { return m > kPanel ? (size_t)m * kPanel : 0; }
+// Elements of side buffer team_invert needs for an m x m block: the new
+// column panel W (m x PW, leading dimension PW) and the scaled row panel R
+// (PW x m, leading dimension m), for the widest panel PW = 64.
+__host__ __device__ inline size_t invert_side_elems(int m) { return m > kGjMax ? 2 * (size_t)m * 64 : 0; }
 
-// Inverts the m x m block at a (lda) in place with the whole team.  W is a side
-// buffer of invert_side_elems(m) elements.  Starts and ends with the block
-// visible to the whole team (the caller synchronised before; this function
-// synchronises after).  Returns false when a team barrier gave up.
-template <class T, int BM, int BN, class Team>
-__device__ bool team_invert(Team& team, T* a, int lda, int m, T* W, int* status, T* smem) {
-  if (m <= kPanel) {
+// Inverts the m x m block at a (lda) in place with the whole team.  `side` holds
+// invert_side_elems(m) elements.  Starts and ends with the block visible to the
+// whole team (the caller synchronised before; this function synchronises
+// after).  Returns false when a team barrier gave up.
+//
+// Per kPanel-wide panel K (rows/columns K0 .. K0+kb):
+//   phase 1: D = A[K,K]^{-1} in place (one CTA); write back the previous
+//            panel's W and R (they were read by the previous phase 3)
+//   phase 2: R[K, J] = D A[K, J] for J outside K        (out of place: no tile
+//            of the product reads what another tile writes)
+//   phase 3: A[I, J] -= A[I, K] R[K, J],  W[I] = -A[I, K] D   for I, J outside K
+template <class T, int BM, int BN, int PW = kPanelRgf, class Team>
+__device__ bool team_invert(Team& team, T* a, int lda, int m, T* side, int* status, T* smem) {
+  if (m <= kGjMax) {
     if (team.rank() == 0) cta_gj_invert<T>(a, lda, m, status, smem);
     return team.sync();
   }
-  const int np = (m + kPanel - 1) / kPanel;
-  int prevK0 = -1, prevkb = 0;
+  T* W = side;                       // m x PW
+  T* R = side + (size_t)m * PW;      // PW x m, leading dimension m
+  const int np = (m + PW - 1) / PW;
+  int pK0 = -1, pkb = 0;
+  auto write_back = [&]() {
+    const int r1 = pK0 + pkb;
+    team_copy<T>(team, pK0, pkb, W, PW, a + pK0, lda);
+    team_copy<T>(team, m - r1, pkb, W + (size_t)r1 * PW, PW, a + (size_t)r1 * lda + pK0, lda);
+    team_copy<T>(team, pkb, pK0, R, m, a + (size_t)pK0 * lda, lda);
+    team_copy<T>(team, pkb, m - r1, R + r1, m, a + (size_t)pK0 * lda + r1, lda);
+  };
   for (int p = 0; p < np; p++) {
-    const int K0 = p * kPanel, kb = min(kPanel, m - K0);
+    const int K0 = p * PW, kb = min(PW, m - K0), right = K0 + kb;
     T* Dinv = a + (size_t)K0 * lda + K0;
-    // (1) invert the pivot block; copy back the previous column panel
     if (team.rank() == 0) cta_gj_invert<T>(Dinv, lda, kb, status, smem);
-    if (prevK0 >= 0) {
-      // rows above and below the previous panel
-      team_copy<T>(team, prevK0, prevkb, W, kPanel, a + prevK0, lda);
-      int r1 = prevK0 + prevkb;
-      team_copy<T>(team, m - r1, prevkb, W + (size_t)r1 * kPanel, kPanel, a + (size_t)r1 * lda + prevK0, lda);
-    }
+    if (pK0 >= 0) write_back();
     if (!team.sync()) return false;
-    // (2) row panel: A[K, J] <- Dinv * A[K, J], J left / right of the panel
     {
       GemmOp<T> ops[2];
-      int right = K0 + kb;
-      ops[0] = make_op<T>(kb, K0, kb, 1.0, Dinv, lda, a + (size_t)K0 * lda, lda, nullptr, 0,
-                          a + (size_t)K0 * lda, lda);
+      ops[0] = make_op<T>(kb, K0, kb, 1.0, Dinv, lda, a + (size_t)K0 * lda, lda, nullptr, 0, R, m);
       ops[1] = make_op<T>(kb, m - right, kb, 1.0, Dinv, lda, a + (size_t)K0 * lda + right, lda, nullptr, 0,
-                          a + (size_t)K0 * lda + right, lda);
+                          R + right, m);
       team_gemm<T, BM, BN>(team, ops, 2, smem);
     }
     if (!team.sync()) return false;
-    // (3) A[I, J] -= A[I, K] A[K, J] for I, J outside the panel; W[I] = -A[I, K] Dinv
     {
       GemmOp<T> ops[6];
-      int right = K0 + kb;
       int rs[2] = {0, right}, rn[2] = {K0, m - right};
       int q = 0;
       for (int ri = 0; ri < 2; ri++) {
         const T* colK = a + (size_t)rs[ri] * lda + K0;
         for (int ci = 0; ci < 2; ci++) {
-          const T* rowK = a + (size_t)K0 * lda + rs[ci];
           T* C = a + (size_t)rs[ri] * lda + rs[ci];
-          ops[q++] = make_op<T>(rn[ri], rn[ci], kb, -1.0, colK, lda, rowK, lda, C, lda, C, lda);
+          ops[q++] = make_op<T>(rn[ri], rn[ci], kb, -1.0, colK, lda, R + rs[ci], m, C, lda, C, lda);
         }
         ops[q++] = make_op<T>(rn[ri], kb, kb, -1.0, colK, lda, Dinv, lda, nullptr, 0,
-                              W + (size_t)rs[ri] * kPanel, kPanel);
+                              W + (size_t)rs[ri] * PW, PW);
       }
       team_gemm<T, BM, BN>(team, ops, q, smem);
     }
     if (!team.sync()) return false;
-    prevK0 = K0;
-    prevkb = kb;
+    pK0 = K0;
+    pkb = kb;
   }
-  team_copy<T>(team, prevK0, prevkb, W, kPanel, a + prevK0, lda);
-  int r1 = prevK0 + prevkb;
-  team_copy<T>(team, m - r1, prevkb, W + (size_t)r1 * kPanel, kPanel, a + (size_t)r1 * lda + prevK0, lda);
+  write_back();
   return team.sync();
 }
 

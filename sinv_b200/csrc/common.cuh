@@ -78,16 +78,15 @@ struct WsHeader {
   unsigned long long desc_offset;
   unsigned long long slots_offset;
   int* inst_status;           // caller's per-instance status array (may be null)
-  unsigned int pad[48];
+  unsigned long long items_offset;
+  int total_slots;            // sum of team sizes
+  unsigned int pad[45];
 };
 static_assert(sizeof(WsHeader) == 256, "header is 256 bytes");
 
 // First failure wins; later ones keep the first code.
 __device__ __forceinline__ void report(int* status, int code) { atomicCAS(status, 0, code); }
 
-// Iteration bound of every spin-wait: ~2^24 polls with backoff is well over a
-// second on B200 and far below any watchdog.
-constexpr unsigned kSpinLimit = 1u << 24;
 
 // ---------------------------------------------------------------------------
 // Teams: the set of CTAs that cooperate on one matrix.  A team splits each
@@ -123,31 +122,57 @@ struct TeamCluster {
   }
 };
 
-// All CTAs of a cooperative launch.  The barrier counts arrivals in the
-// workspace header; generation g waits for (g+1) * size arrivals.
-struct TeamGrid {
-  WsHeader* hdr;
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Upper bound of every team-barrier wait.  Team members may join late (a
+// CTA finishes its previous instance first), so the bound is generous; a wait
+// that reaches it reports SINVB_STATUS_TIMEOUT and the team abandons the work.
+constexpr unsigned long long kTeamWaitNs = 60ull * 1000000000ull;
+
+// A team of `n` CTAs that meet at a counter in global memory: the CTAs of a
+// cooperative launch (the whole GPU on one matrix) or the members of one
+// batched work item.  Generation g waits for (g+1) * n arrivals.  All members
+// are resident (persistent or cooperative launches), so every wait ends.
+struct TeamDyn {
+  unsigned* counter;
+  int* status;
+  int r, n;
   unsigned generation;
-  __device__ int rank() const { return blockIdx.x; }
-  __device__ int size() const { return gridDim.x; }
+  __device__ int rank() const { return r; }
+  __device__ int size() const { return n; }
   __device__ bool sync() {
+    if (n == 1) {
+      __syncthreads();
+      return true;
+    }
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-      unsigned target = (generation + 1) * gridDim.x;
+      const unsigned target = (generation + 1) * (unsigned)n;
       __threadfence();
-      atomicAdd(&hdr->barrier_count, 1u);
-      unsigned spins = 0, seen;
+      atomicAdd(counter, 1u);
+      unsigned seen;
       int good = 1;
-      while (true) {
-        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(&hdr->barrier_count) : "memory");
+      unsigned long long t0 = 0;
+      for (unsigned spins = 0;; spins++) {
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(counter) : "memory");
         if (seen >= target) break;
-        if (++spins > kSpinLimit) {
-          report(&hdr->status, SINVB_STATUS_TIMEOUT);
-          good = 0;
-          break;
+        if (spins > 64) {
+          __nanosleep(64);
+          if ((spins & 1023) == 0) {
+            unsigned long long now = global_ns();
+            if (t0 == 0) t0 = now;
+            else if (now - t0 > kTeamWaitNs) {
+              report(status, SINVB_STATUS_TIMEOUT);
+              good = 0;
+              break;
+            }
+          }
         }
-        if (spins > 64) __nanosleep(32);
       }
       __threadfence();
       ok = good;

@@ -109,12 +109,15 @@ extern "C" int sinvb_rgf_z_noalloc(const void* diag, const void* upper, const vo
   p.P = p.Gu;
   p.T0 = reinterpret_cast<cplx*>(s + sizeof(WsHeader));
   p.T1 = p.T0 + (size_t)b * b;
+  p.T2 = p.T3 = nullptr;  // in-place mode only
   p.Winv = nullptr;  // blocks of at most 64 x 64 invert without the side buffer
   p.hdr = reinterpret_cast<WsHeader*>(s);
   p.status = &p.hdr->status;
   p.n = n;
   p.b = b;
   p.flags = flags;
+  p.ckpt = nullptr;
+  p.ckpt_every = 1;
   if (b <= 32) return launch_noalloc<32, 32>(p, status, st);
   return launch_noalloc<64, 64>(p, status, st);
 }

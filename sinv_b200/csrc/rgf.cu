@@ -24,7 +24,7 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_cta_kernel(RgfParams<T> p) {
 template <class T, int BM, int BN>
 __global__ void __launch_bounds__(kThreads, 1) rgf_grid_kernel(RgfParams<T> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  TeamGrid team{p.hdr, 0};
+  TeamDyn team{&p.hdr->barrier_count, p.status, (int)blockIdx.x, (int)gridDim.x, 0u};
   rgf_sweep<T, BM, BN>(team, p, reinterpret_cast<T*>(smem_raw));
 }
 
@@ -46,7 +46,7 @@ constexpr size_t sweep_smem_bytes() {
 }
 
 struct RgfLayout {
-  size_t X, P, T0, T1, Winv, wide_in, wide_out, total;
+  size_t X, P, T0, T1, T2, T3, Winv, wide_in, wide_out, total;
 };
 
 // Workspace layout (bytes, 256-aligned pieces after the 256-byte header).
@@ -67,6 +67,10 @@ static RgfLayout rgf_layout(int n, int b, int dtype, unsigned flags) {
   }
   L.T0 = take(bb * es);
   L.T1 = take(bb * es);
+  if (flags & SINVB_INPLACE) {
+    L.T2 = take(bb * es);
+    L.T3 = take(bb * es);
+  }
   L.Winv = take(invert_side_elems(b) * es);
   if (dtype == SINVB_C64 || dtype == SINVB_F32) {
     L.wide_in = take((size_t)(3 * n - 2) * bb * es);
@@ -105,19 +109,27 @@ static bool use_grid_team(int b, unsigned flags) {
 
 template <class T>
 static int run_rgf(const T* diag, const T* upper, const T* lower, int n, int b, unsigned flags, T* Gd, T* Gu,
-                   T* Gl, unsigned char* ws, const RgfLayout& L, cudaStream_t stream) {
+                   T* Gl, unsigned char* ws, const RgfLayout& L, cudaStream_t stream, T* ckpt = nullptr,
+                   int ckpt_every = 1) {
   RgfParams<T> p;
+  p.ckpt = ckpt;
+  p.ckpt_every = ckpt_every;
   p.diag = diag;
   p.upper = upper;
   p.lower = lower;
-  p.Gd = Gd;
-  p.Gu = Gu;
-  p.Gl = Gl;
+  const bool inplace = flags & SINVB_INPLACE;
+  p.Gd = inplace ? const_cast<T*>(diag) : Gd;
+  p.Gu = inplace ? const_cast<T*>(upper) : Gu;
+  p.Gl = inplace ? const_cast<T*>(lower) : Gl;
+  Gu = p.Gu;
+  Gl = p.Gl;
   const bool save = flags & SINVB_SAVE_OFFDIAG;
   p.X = save ? Gl : reinterpret_cast<T*>(ws + L.X);
   p.P = save ? Gu : reinterpret_cast<T*>(ws + L.P);
   p.T0 = reinterpret_cast<T*>(ws + L.T0);
   p.T1 = reinterpret_cast<T*>(ws + L.T1);
+  p.T2 = inplace ? reinterpret_cast<T*>(ws + L.T2) : nullptr;
+  p.T3 = inplace ? reinterpret_cast<T*>(ws + L.T3) : nullptr;
   p.Winv = reinterpret_cast<T*>(ws + L.Winv);
   p.hdr = reinterpret_cast<WsHeader*>(ws);
   p.status = &p.hdr->status;
@@ -132,9 +144,12 @@ static int run_rgf(const T* diag, const T* upper, const T* lower, int n, int b, 
 
 static int check_args(const void* diag, const void* upper, const void* lower, int n, int b, unsigned flags,
                       const void* Gd, const void* Gu, const void* Gl, const void* ws, size_t ws_bytes, int dtype) {
-  if (n < 1 || b < 1 || !diag || !Gd || !ws) return SINVB_EINVAL;
+  const bool inplace = flags & SINVB_INPLACE;
+  if (n < 1 || b < 1 || !diag || !ws) return SINVB_EINVAL;
+  if (!inplace && !Gd) return SINVB_EINVAL;
   if (n > 1 && (!upper || !lower)) return SINVB_EINVAL;
-  if ((flags & SINVB_SAVE_OFFDIAG) && n > 1 && (!Gu || !Gl)) return SINVB_EINVAL;
+  if (!inplace && (flags & SINVB_SAVE_OFFDIAG) && n > 1 && (!Gu || !Gl)) return SINVB_EINVAL;
+  if (inplace && (!(flags & SINVB_SAVE_OFFDIAG) || dtype == SINVB_C64 || dtype == SINVB_F32)) return SINVB_EINVAL;
   if ((flags & SINVB_FORCE_GRID) && (flags & SINVB_FORCE_CTA)) return SINVB_EINVAL;
   if ((uintptr_t)ws % 256 != 0) return SINVB_EWORKSPACE;
   if (ws_bytes < rgf_layout(n, b, dtype, flags).total) return SINVB_EWORKSPACE;
@@ -225,6 +240,37 @@ int sinvb_rgf_s(const void* diag, const void* upper, const void* lower, int n, i
                 sinvb_stream_t stream) {
   return rgf_single<double>(diag, upper, lower, n, b, flags, G_diag, G_upper, G_lower, workspace, workspace_bytes,
                             (cudaStream_t)stream, SINVB_F32);
+}
+
+}  // extern "C"
+
+// Forward sweep that also saves the adjoint's checkpoints g_{s*c-1} -> ckpt[s-1].
+template <class T>
+static int rgf_ckpt(const void* diag, const void* upper, const void* lower, int n, int b, unsigned flags,
+                    void* G_diag, void* G_upper, void* G_lower, void* ckpt, int every, void* workspace,
+                    size_t workspace_bytes, cudaStream_t stream, int dtype) {
+  if (!(flags & SINVB_SAVE_OFFDIAG) || (flags & SINVB_INPLACE) || every < 1) return SINVB_EINVAL;
+  if ((n - 1) / every >= 1 && !ckpt) return SINVB_EINVAL;
+  int rc = check_args(diag, upper, lower, n, b, flags, G_diag, G_upper, G_lower, workspace, workspace_bytes, dtype);
+  if (rc) return rc;
+  return run_rgf<T>((const T*)diag, (const T*)upper, (const T*)lower, n, b, flags, (T*)G_diag, (T*)G_upper,
+                    (T*)G_lower, (unsigned char*)workspace, rgf_layout(n, b, dtype, flags), stream, (T*)ckpt, every);
+}
+
+extern "C" {
+
+int sinvb_rgf_forward_ckpt_z(const void* diag, const void* upper, const void* lower, int n, int b, unsigned flags,
+                             void* G_diag, void* G_upper, void* G_lower, void* checkpoints, int every,
+                             void* workspace, size_t workspace_bytes, sinvb_stream_t stream) {
+  return rgf_ckpt<cplx>(diag, upper, lower, n, b, flags, G_diag, G_upper, G_lower, checkpoints, every, workspace,
+                        workspace_bytes, (cudaStream_t)stream, SINVB_C128);
+}
+
+int sinvb_rgf_forward_ckpt_d(const void* diag, const void* upper, const void* lower, int n, int b, unsigned flags,
+                             void* G_diag, void* G_upper, void* G_lower, void* checkpoints, int every,
+                             void* workspace, size_t workspace_bytes, sinvb_stream_t stream) {
+  return rgf_ckpt<double>(diag, upper, lower, n, b, flags, G_diag, G_upper, G_lower, checkpoints, every, workspace,
+                          workspace_bytes, (cudaStream_t)stream, SINVB_F64);
 }
 
 }  // extern "C"

@@ -22,6 +22,11 @@
 // G_lower[i] and P_{i+1} in G_upper[i] until the backward step overwrites
 // them; otherwise both live in the workspace.  T alternates between two
 // workspace blocks and is copied to G_lower[i] one phase later.
+//
+// In place (SINVB_INPLACE): G_diag, G_upper, G_lower are the input arrays.
+// A_{i,i-1} is dead after F1 of step i and A_{i-1,i} after F2, so X_{i-1} and
+// P_i are first written to a pair of workspace blocks (alternating between
+// two pairs by step parity) and copied over the dead inputs one phase later.
 #pragma once
 
 #include "block_inverse.cuh"
@@ -40,11 +45,15 @@ struct RgfParams {
   T* P;    // n-1 blocks (may alias Gu)
   T* T0;   // b*b
   T* T1;   // b*b
+  T* T2;   // b*b (in place only)
+  T* T3;   // b*b (in place only)
   T* Winv; // invert_side_elems(b)
   WsHeader* hdr;   // grid-team barrier counter (unused by other teams)
   int* status;     // device status word of this matrix
   int n, b;
   unsigned flags;
+  T* ckpt;         // optional: g_{s*c-1} saved to ckpt[s-1] (s = 1, 2, ...) for the adjoint
+  int ckpt_every;  // c
 };
 
 template <class T, int BM, int BN, class Team>
@@ -54,29 +63,45 @@ __device__ void rgf_sweep(Team& team, const RgfParams<T>& p, T* smem) {
   const bool sym = p.flags & SINVB_SYM;
   const bool save = p.flags & SINVB_SAVE_OFFDIAG;
 
+  const bool inplace = p.flags & SINVB_INPLACE;
+
   // g_0 = A_00^{-1}
-  team_copy<T>(team, b, b, p.diag, b, p.Gd, b);
-  if (!team.sync()) return;
+  if (!inplace) {
+    team_copy<T>(team, b, b, p.diag, b, p.Gd, b);
+    if (!team.sync()) return;
+  }
   if (!team_invert<T, BM, BN>(team, p.Gd, b, b, p.Winv, p.status, smem)) return;
 
   for (int i = 1; i < n; i++) {
     const T* g = p.Gd + (i - 1) * bb;
     const T* U = p.upper + (i - 1) * bb;
     const T* L = p.lower + (i - 1) * bb;
+    // in place: X_{i-1} / P_i go to a temp pair, alternating by parity
+    T* Xd = inplace ? ((i & 1) ? p.T2 : p.T0) : p.X + (i - 1) * bb;
+    T* Pd = inplace ? ((i & 1) ? p.T3 : p.T1) : p.P + (i - 1) * bb;
     {  // F1
       GemmOp<T> ops[2];
-      ops[0] = make_op<T>(b, b, b, 1.0, g, b, U, b, nullptr, 0, p.X + (i - 1) * bb, b);
-      ops[1] = make_op<T>(b, b, b, 1.0, L, b, g, b, nullptr, 0, p.P + (i - 1) * bb, b);
+      ops[0] = make_op<T>(b, b, b, 1.0, g, b, U, b, nullptr, 0, Xd, b);
+      ops[1] = make_op<T>(b, b, b, 1.0, L, b, g, b, nullptr, 0, Pd, b);
       team_gemm<T, BM, BN>(team, ops, 2, smem);
+      if (inplace && i >= 2)  // P_{i-1} over A_{i-2,i-1}, dead since F2 of step i-1
+        team_copy<T>(team, b, b, (i & 1) ? p.T1 : p.T3, b, p.Gu + (i - 2) * bb, b);
+      if (p.ckpt && i % p.ckpt_every == 0)  // checkpoint g_{i-1} for the adjoint
+        team_copy<T>(team, b, b, g, b, p.ckpt + (size_t)(i / p.ckpt_every - 1) * bb, b);
     }
     if (!team.sync()) return;
     {  // F2: S_i = A_ii - P_i U_{i-1}
-      GemmOp<T> op = make_op<T>(b, b, b, -1.0, p.P + (i - 1) * bb, b, U, b, p.diag + i * bb, b,
-                                p.Gd + i * bb, b);
+      GemmOp<T> op = make_op<T>(b, b, b, -1.0, Pd, b, U, b, p.diag + i * bb, b, p.Gd + i * bb, b);
       team_gemm<T, BM, BN>(team, &op, 1, smem);
+      if (inplace)  // X_{i-1} over A_{i,i-1}, dead since F1
+        team_copy<T>(team, b, b, Xd, b, p.Gl + (i - 1) * bb, b);
     }
     if (!team.sync()) return;
     if (!team_invert<T, BM, BN>(team, p.Gd + i * bb, b, b, p.Winv, p.status, smem)) return;
+  }
+  if (inplace && n >= 2) {
+    team_copy<T>(team, b, b, ((n - 1) & 1) ? p.T3 : p.T1, b, p.Gu + (n - 2) * bb, b);
+    if (!team.sync()) return;
   }
 
   T* prevT = nullptr;

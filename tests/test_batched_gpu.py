@@ -101,3 +101,24 @@ def test_singular_instance_reported_by_index():
     good = plan.results(like=inst[0][0])
     for k in (0, 1, 3):
         _check(good[k], rgf_oracle.rgf(*inst[k]), 1e-12)
+
+
+@pytest.mark.parametrize("inplace", [False, True])
+def test_teams_for_large_blocks_and_in_place(inplace):
+    """b = 256 / 512 instances run on teams of 2 / 4 CTAs; optionally in place."""
+    import torch
+    shapes = [(3, 512), (2, 256), (4, 64), (3, 256), (1, 512), (5, 32)]
+    inst = [workloads.dominant(n, b, seed=200 + k) for k, (n, b) in enumerate(shapes)]
+    tinst = [tuple(torch.from_numpy(x).cuda() for x in t) for t in inst]
+    plan = BatchPlan(tinst, inplace=inplace)
+    plan.run()
+    plan.check()
+    for (d, u, l), G in zip(inst, plan.results()):
+        _check([g.cpu().numpy() for g in G], rgf_oracle.rgf(d, u, l), 1e-12)
+    if inplace:
+        assert plan.results()[0][0].data_ptr() == tinst[0][0].data_ptr()
+    single = BatchPlan([tuple(torch.from_numpy(x).cuda() for x in t) for t in inst], team="cta")
+    single.run()
+    for G1, G2 in zip(plan.results(), single.results()):
+        for a, b in zip(G1, G2):
+            assert _rel(a.cpu().numpy(), b.cpu().numpy()) <= 1e-12

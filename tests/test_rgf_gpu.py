@@ -115,3 +115,13 @@ def test_at_scale_plain_matches_oracle(n, b):
     d, u, l = workloads.dominant(n, b, seed=0)
     G = rgf.rgf(d, u, l)
     _check(G, rgf_oracle.rgf(d, u, l), TOL_PLAIN)
+
+
+@pytest.mark.parametrize("n,b,team", [(1, 8, None), (2, 16, None), (7, 33, None), (6, 70, "grid"), (4, 130, None)])
+def test_overwrite_a_in_place(n, b, team):
+    import torch
+    d, u, l = workloads.dominant(n, b, seed=9 + n)
+    td, tu, tl = (torch.from_numpy(x).cuda() for x in (d, u, l))
+    G = rgf.rgf_blocks(td, tu, tl, overwrite_a=True, team=team)
+    assert G[0].data_ptr() == td.data_ptr()
+    _check([g.cpu().numpy() for g in G], rgf_oracle.rgf(d, u, l), TOL_PLAIN)
