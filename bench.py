@@ -168,6 +168,21 @@ def fp64_peak_tflops(torch):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def dmma_peak_tflops(torch):
+    """Measured FP64 tensor-core (DMMA) peak of this GPU, best of 3 probe runs."""
+    import ctypes
+    from sinv_b200 import _lib
+    lib = _lib.load()
+    best = 0.0
+    for _ in range(3):
+        v = ctypes.c_double(0.0)
+        _lib.check(lib.sinvb_fp64_mma_peak(1 << 16, ctypes.byref(v),
+                                           ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)),
+                   "sinvb_fp64_mma_peak")
+        best = max(best, v.value)
+    return best
+
+
 def cpu_sample(spec):
     """Stratified CPU sample: the first instance of each block size."""
     seen, idx = set(), []
@@ -243,7 +258,8 @@ def run_sinvb(args, rank, world, local_rank):
     torch.cuda.set_device(dev)
     shape = tuple(int(x) for x in args.shape.split(",")) if args.shape else None
     spec = batch_spec(args.count, rank, shape)
-    peak = fp64_peak_tflops(torch)
+    dgemm_peak = fp64_peak_tflops(torch)
+    peak = dmma_peak_tflops(torch)
 
     free, _ = torch.cuda.mem_get_info()
     # In place (results over the inputs): the whole batch fits in HBM as one
@@ -322,8 +338,9 @@ def run_sinvb(args, rank, world, local_rank):
            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                         "frac": achieved / peak, "traffic": None,
                         "kernel": "rgf_batched_kernel", "flops": "canonical 8 b^3 (8(n-1)+n) per instance",
-                        "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured at start on this GPU "
-                                       "(no FP64 figure in MEASURED_PEAKS.json)"},
+                        "peak_source": "FP64 tensor-core (DMMA) rate measured at start on this GPU by "
+                                       "sinvb_fp64_mma_peak (MEASURED_PEAKS.json has no FP64 figure)",
+                        "peak_dgemm_cublas": dgemm_peak},
            "clocks": clk}
     if acc is not None:
         out["rel_err_vs_fp64"] = acc

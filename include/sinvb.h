@@ -190,6 +190,32 @@ int sinvb_rgf_batched_d(const sinvb_batch_desc* descs, int count, unsigned flags
 int sinvb_rgf_batched_rerun_z(void* workspace, sinvb_stream_t stream);
 int sinvb_rgf_batched_rerun_d(void* workspace, sinvb_stream_t stream);
 
+/* ---- mixed-precision complex GEMM on the int8 tensor cores ---------------------- */
+/*
+ * No reference counterpart (the reference multiplies blocks with numpy/BLAS
+ * zgemm, src/sinv/algorithms/rgf/rgf.py:48,53,60,62); the block product of
+ * the mixed-precision sweeps, exposed on its own.  C = beta D + alpha A B for
+ * row-major complex128 A (M x K), B (K x N), D, C (M x N), computed by the
+ * Ozaki scheme on tcgen05.mma kind::i8: per-row / per-column power-of-two
+ * scaling, `digits` signed 7-bit slices per value (1..8), exact int32
+ * accumulation; error ~ 2^-(7*digits-1) relative to |A||B|.  D may be NULL.
+ * Requires 2K <= 16384.
+ */
+size_t sinvb_zgemm_ozaki_workspace_size(int M, int N, int K, int digits);
+int sinvb_zgemm_ozaki(int M, int N, int K, double alpha, const void* A, int lda, const void* B, int ldb,
+                      double beta, const void* D, int ldd, void* C, int ldc, int digits, void* workspace,
+                      size_t workspace_bytes, sinvb_stream_t stream);
+
+/* ---- diagnostics ------------------------------------------------------------- */
+/*
+ * No reference counterpart: measures the FP64 tensor-core (DMMA) rate of the
+ * current device, the ceiling of every FP64 kernel here (B200 has no FP64
+ * kind of tcgen05.mma).  Runs `iters` dependent-free mma.sync.m8n8k4.f64
+ * steps in 8 chains per warp, 8 warps per CTA, 2 CTAs per SM, timed with CUDA
+ * events on `stream` (synchronises it).  Result in TFLOP/s.
+ */
+int sinvb_fp64_mma_peak(int iters, double* tflops, sinvb_stream_t stream);
+
 /* ---- allocation-free variant ------------------------------------------------ */
 /*
  * No counterpart in the reference.  For callers that cannot allocate device

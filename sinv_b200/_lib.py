@@ -57,6 +57,10 @@ SIGNATURES = {
     "sinvb_rgf_adjoint_workspace_size": (_sz, [_i, _i, _i, _u]),
     "sinvb_rgf_adjoint_z": (_i, [_vp] * 10 + [_i, _i, _i, _u, _vp, _vp, _vp, _vp, _sz, _vp]),
     "sinvb_rgf_adjoint_d": (_i, [_vp] * 10 + [_i, _i, _i, _u, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "sinvb_fp64_mma_peak": (_i, [_i, ctypes.POINTER(ctypes.c_double), _vp]),
+    "sinvb_zgemm_ozaki_workspace_size": (_sz, [_i, _i, _i, _i]),
+    "sinvb_zgemm_ozaki": (_i, [_i, _i, _i, ctypes.c_double, _vp, _i, _vp, _i, ctypes.c_double, _vp, _i, _vp, _i,
+                               _i, _vp, _sz, _vp]),
     "sinvb_bcr_workspace_size": (_sz, [_i, _i, _i, _u]),
     "sinvb_bcr_z": (_i, _RGF_ARGS),
     "sinvb_bcr_d": (_i, _RGF_ARGS),

@@ -76,7 +76,7 @@ constexpr int kStages = 3;
 
 template <class T> struct GemmCfg;
 template <> struct GemmCfg<cplx> {
-  static constexpr int BK = 8;
+  static constexpr int BK = 16;
   __device__ static int a_idx(int m, int k) { return m * BK + (k ^ ((m & 1) << 2)); }
   template <int BN> __device__ static int b_idx(int k, int n) { return k * BN + (n ^ ((k & 3) << 1)); }
 };
@@ -166,13 +166,20 @@ __device__ __forceinline__ void mma_chunk(const cplx* sA, const cplx* sB, double
       b[nt].re *= sbr;
       b[nt].im *= sbi;
     }
+    // Two passes so that the two products landing on the same accumulator are
+    // MT*NT*2 instructions apart instead of back to back (DMMA latency).
 #pragma unroll
     for (int mt = 0; mt < W::MT; mt++)
 #pragma unroll
       for (int nt = 0; nt < W::NT; nt++) {
         dmma884(acc[mt][nt][0], acc[mt][nt][1], a[mt].re, b[nt].re);
-        dmma884(acc[mt][nt][0], acc[mt][nt][1], a[mt].im, -b[nt].im);
         dmma884(acc[mt][nt][2], acc[mt][nt][3], a[mt].re, b[nt].im);
+      }
+#pragma unroll
+    for (int mt = 0; mt < W::MT; mt++)
+#pragma unroll
+      for (int nt = 0; nt < W::NT; nt++) {
+        dmma884(acc[mt][nt][0], acc[mt][nt][1], a[mt].im, -b[nt].im);
         dmma884(acc[mt][nt][2], acc[mt][nt][3], a[mt].im, b[nt].re);
       }
   }

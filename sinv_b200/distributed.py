@@ -1,0 +1,124 @@
+"""One process per GPU: sharding the energy loop across ranks.
+
+A transport calculation solves one selected inversion per energy point.  The
+points are independent, so they shard across GPUs with no exchange during the
+sweeps: every rank takes a cost-balanced share (cost ~ b^3 n per instance),
+runs it as one batched launch, and only the quantities that are sums over
+energies (the density of states, the gradient dL/dH of an energy-summed loss)
+cross ranks, as one all-reduce at the end.  Launch with torchrun, one rank per
+GPU, backend ``nccl`` (``gloo`` for CPU tests).
+"""
+
+import heapq
+
+import numpy as np
+
+
+def instance_cost(n, b):
+    """Relative cost of one selected inversion: the canonical flop count."""
+    return float(b) ** 3 * (9 * n - 8)
+
+
+def shard_by_cost(costs, world, rank=None):
+    """Largest-first greedy partition of instances into ``world`` bins.
+
+    Deterministic (ties broken by index), so every rank computes the same
+    plan without communicating.  Returns the index list of ``rank`` or, with
+    ``rank=None``, all ranks' lists.
+    """
+    order = sorted(range(len(costs)), key=lambda k: (-costs[k], k))
+    heap = [(0.0, r) for r in range(world)]
+    bins = [[] for _ in range(world)]
+    for k in order:
+        load, r = heapq.heappop(heap)
+        bins[r].append(k)
+        heapq.heappush(heap, (load + costs[k], r))
+    for b in bins:
+        b.sort()
+    return bins if rank is None else bins[rank]
+
+
+def _dist():
+    import torch.distributed as dist
+    return dist
+
+
+def rank_and_world(group=None):
+    dist = _dist()
+    if dist.is_available() and dist.is_initialized():
+        return dist.get_rank(group), dist.get_world_size(group)
+    return 0, 1
+
+
+def rgf_batched_sharded(instances, group=None, **kw):
+    """Batched RGF of this rank's share of ``instances`` (all ranks pass the
+    same list).  Returns ``{index: (G_diag, G_upper, G_lower)}`` for the
+    instances this rank computed."""
+    from .algorithms.batched import rgf_batched
+    rank, world = rank_and_world(group)
+    costs = [instance_cost(np.shape(d)[0], np.shape(d)[1]) for d, _, _ in instances]
+    mine = shard_by_cost(costs, world, rank)
+    if not mine:
+        return {}
+    out = rgf_batched([instances[k] for k in mine], **kw)
+    return dict(zip(mine, out))
+
+
+def energy_loss_and_grad(H_onsite, H_coupling, energies, eta=1e-3, sigma=0.1, group=None, compute=None):
+    """Sum over energies of L(E) = -Im Tr sum_i G_ii(E) / pi and its gradient
+    with respect to the Hamiltonian blocks, sharded over ranks.
+
+    ``A(E) = (E + i eta) I - H - Sigma`` with ``Sigma = -i sigma I`` on the
+    first and last diagonal blocks; H onsite blocks (n, b, b), couplings
+    (n-1, b, b) above the diagonal and their transposes below.  Each rank
+    evaluates its share of the energies (``compute(E) -> (loss, g_onsite,
+    g_coupling)``, by default the GPU adjoint) and one all-reduce sums the
+    loss and both gradients.  Returns ``(loss, g_onsite, g_coupling)`` as torch
+    tensors on the inputs' device, identical on every rank.
+    """
+    import torch
+    dist = _dist()
+    rank, world = rank_and_world(group)
+    n, b = H_onsite.shape[0], H_onsite.shape[1]
+    mine = shard_by_cost([1.0] * len(energies), world, rank)
+    if compute is None:
+        compute = _gpu_energy_term(H_onsite, H_coupling, eta, sigma)
+    loss = torch.zeros((), dtype=torch.float64, device=H_onsite.device)
+    g_on = torch.zeros_like(H_onsite, dtype=torch.float64)
+    g_cp = torch.zeros_like(H_coupling, dtype=torch.float64)
+    for k in mine:
+        l_k, go, gc = compute(float(energies[k]))
+        loss += l_k
+        g_on += go
+        g_cp += gc
+    if world > 1:
+        flat = torch.cat([loss.reshape(1), g_on.reshape(-1), g_cp.reshape(-1)])
+        dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=group)
+        loss = flat[0]
+        g_on = flat[1:1 + g_on.numel()].view_as(g_on)
+        g_cp = flat[1 + g_on.numel():].view_as(g_cp)
+    return loss, g_on, g_cp
+
+
+def _gpu_energy_term(H_onsite, H_coupling, eta, sigma):
+    import torch
+    from .algorithms.adjoint import rgf_autograd
+
+    def term(E):
+        Hd = H_onsite.detach().clone().requires_grad_(True)
+        Hu = H_coupling.detach().clone().requires_grad_(True)
+        b = Hd.shape[1]
+        eye = torch.eye(b, dtype=torch.complex128, device=Hd.device)
+        d = (E + 1j * eta) * eye - Hd.to(torch.complex128)
+        edge = torch.zeros_like(d)
+        edge[0] = 1j * sigma * eye
+        edge[-1] = edge[-1] + 1j * sigma * eye
+        d = d + edge
+        u = -Hu.to(torch.complex128)
+        l = -Hu.transpose(1, 2).to(torch.complex128)
+        Gd, _, _ = rgf_autograd(d, u.contiguous(), l.contiguous())
+        loss = -Gd.diagonal(0, 1, 2).imag.sum() / np.pi
+        loss.backward()
+        return loss.detach(), Hd.grad, Hu.grad
+
+    return term

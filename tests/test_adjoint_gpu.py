@@ -50,7 +50,7 @@ def grads(fn, d, u, l, w):
     leaves = [x.clone().requires_grad_(True) for x in (d, u, l)]
     loss = loss_fn(*fn(*leaves), *w)
     loss.backward()
-    return [x.grad for x in leaves], loss.item()
+    return [x.grad if x.grad is not None else torch.zeros_like(x) for x in leaves], loss.item()
 
 
 def rel(a, b):
@@ -127,8 +127,9 @@ def test_adjoint_central_finite_differences():
             Lp = loss_fn(*rgf_autograd(d + h * V[0], u + h * V[1], l + h * V[2]), *w).item()
             Lm = loss_fn(*rgf_autograd(d - h * V[0], u - h * V[1], l - h * V[2]), *w).item()
         fd = (Lp - Lm) / (2 * h)
-        # dL = 2 Re <grad, dA> for the conjugate-Wirtinger gradient torch returns
-        an = sum(2 * (torch.conj(g) * v).real.sum().item() for g, v in zip((gd, gu, gl), V))
+        # torch's gradient of a real loss w.r.t. a complex tensor z is 2 dL/dz*,
+        # so the directional derivative along v is Re <grad, v>
+        an = sum((torch.conj(g) * v).real.sum().item() for g, v in zip((gd, gu, gl), V))
         assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (fd, an)
 
 
