@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="sinvb", choices=["sinvb", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--digits", type=int, default=7, help="int8 slices per value of the mixed products")
     ap.add_argument("--count", type=int, default=512)
     ap.add_argument("--shape", default=None, help="n,b: uniform batch of that shape instead of the energy batch")
     ap.add_argument("--wave-gb", type=float, default=0.0, help="input GB per wave (0: as much as HBM holds)")
@@ -275,7 +276,8 @@ def run_sinvb(args, rank, world, local_rank):
     pin = torch.empty(pool_elems, dtype=torch.complex128, device=dev)
     plans = []
     for w in waves:
-        plans.append(BatchPlan(carve(pin, spec, w), precision=args.precision, inplace=True))
+        plans.append(BatchPlan(carve(pin, spec, w), precision=args.precision, inplace=True,
+                               digits=args.digits))
     flops = [sum(workloads.rgf_flops(spec[k][1], spec[k][2]) for k in w) for w in waves]
 
     def generate(wi):
@@ -319,11 +321,6 @@ def run_sinvb(args, rank, world, local_rank):
     value = args.count * world / (ms_step * 1e-3)
     achieved = sum(kern_flops) / (sum(kern_ms) * 1e-3) / 1e12
 
-    # accuracy of this precision against the FP64 path, on the first instances
-    acc = None
-    if args.precision != "fp64":
-        acc = "not measured"
-
     workload = WORKLOAD if shape is None else "uniform_%dx(n=%d,b=%d)" % (args.count, shape[0], shape[1])
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -342,8 +339,6 @@ def run_sinvb(args, rank, world, local_rank):
                                        "sinvb_fp64_mma_peak (MEASURED_PEAKS.json has no FP64 figure)",
                         "peak_dgemm_cublas": dgemm_peak},
            "clocks": clk}
-    if acc is not None:
-        out["rel_err_vs_fp64"] = acc
 
     # the plain per-matrix FP64 path (one library call per instance, the whole
     # GPU on each matrix) over the same batch, one pass, same in-place inputs
@@ -365,12 +360,41 @@ def run_sinvb(args, rank, world, local_rank):
 
     del pin, plans, plan   # `plan` (loop variable) holds views of the pool too
     torch.cuda.empty_cache()
+    # accuracy of this precision against the FP64 path, on a sample of the batch
+    if args.precision != "fp64":
+        out["rel_err_vs_fp64"] = mixed_accuracy(torch, spec, args, dev)
     # e2e on a stratified sample (every 16th instance)
     if not args.no_e2e:
         out["e2e"] = e2e_sample(torch, spec, args, dev, world)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(spec)
     return out
+
+
+def mixed_accuracy(torch, spec, args, dev):
+    """Relative Frobenius error of the mixed path against the FP64 path, per
+    output array (G_diag, G_upper, G_lower) of every 32nd instance."""
+    from sinv_b200 import workloads
+    from sinv_b200.algorithms import BatchPlan
+
+    idx = list(range(0, len(spec), 32))
+    inst = [workloads.tight_binding_device(spec[k][1], spec[k][2], spec[k][0], spec[k][3], device=dev)
+            for k in idx]
+    ref = BatchPlan(inst)
+    mix = BatchPlan(inst, precision=args.precision, digits=args.digits)
+    ref.run()
+    mix.run()
+    ref.check()
+    mix.check()
+    errs = []
+    for G, R in zip(mix.results(), ref.results()):
+        for a, r in zip(G, R):
+            if r.numel():
+                errs.append(float(torch.linalg.vector_norm(a - r) / torch.linalg.vector_norm(r)))
+    del ref, mix, inst
+    torch.cuda.empty_cache()
+    return {"max": max(errs), "median": statistics.median(errs), "digits": args.digits,
+            "bar": 1e-8, "sample": "every 32nd instance (%d), each of G_diag/G_upper/G_lower" % len(idx)}
 
 
 def e2e_sample(torch, spec, args, dev, world):
@@ -392,7 +416,7 @@ def e2e_sample(torch, spec, args, dev, world):
     host_in = torch.empty(tot, dtype=torch.complex128, pin_memory=True)
     host_out = torch.empty(tot, dtype=torch.complex128, pin_memory=True)
     host_in.copy_(pin_dev)
-    plan = BatchPlan(ins, outputs=outs, precision=args.precision)
+    plan = BatchPlan(ins, outputs=outs, precision=args.precision, digits=args.digits)
     stream = torch.cuda.current_stream()
     times = []
     for step in range(args.warmup + args.steps):

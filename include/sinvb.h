@@ -170,6 +170,8 @@ typedef struct sinvb_batch_desc {
 /* precision modes of the batched call (the ``flags`` argument, high bits) */
 #define SINVB_PREC_FP64 0u          /* every product in FP64 (DMMA)             */
 #define SINVB_PREC_MIXED (1u << 8)  /* block products on tcgen05, FP64 inverses */
+/* int8 slices per value of the mixed products (1..8) in flag bits 12-15; 0 means 7 */
+#define SINVB_PREC_DIGITS(d) (((unsigned)(d) & 15u) << 12)
 
 size_t sinvb_rgf_batched_workspace_size(const sinvb_batch_desc* descs, int count, int dtype, unsigned flags);
 

@@ -68,6 +68,7 @@ SIGNATURES = {
 
 PREC_FP64 = 0
 PREC_MIXED = 1 << 8
+PREC_DIGITS_SHIFT = 12  # Ozaki digits of the mixed products in flag bits 12-15 (0: 7)
 
 
 class BatchDesc(ctypes.Structure):

@@ -22,12 +22,12 @@
 
 namespace sinvb {
 
-// The instance count of the last upload into a workspace, kept host-side so a
-// re-run needs no device read (the kernel reads everything else from the
-// workspace header).
+// The instance count and flags of the last upload into a workspace, kept
+// host-side so a re-run needs no device read (the kernel reads everything else
+// from the workspace header).
 static std::mutex g_count_mutex;
-static std::unordered_map<const void*, int>& count_table() {
-  static std::unordered_map<const void*, int> t;
+static std::unordered_map<const void*, std::pair<int, unsigned>>& count_table() {
+  static std::unordered_map<const void*, std::pair<int, unsigned>> t;
   return t;
 }
 
@@ -46,6 +46,22 @@ struct BatchEntry {
   int pad[3];
 };
 static_assert(sizeof(BatchEntry<cplx>) == 80, "80-byte entries");
+
+// Digits of the mixed-precision products (flags bits 12-15; 0 means 7).
+__host__ __device__ inline int mixed_digits(unsigned flags) {
+  const int d = (int)((flags >> 12) & 15u);
+  return d == 0 ? 7 : d;
+}
+
+// Bytes of the FP64 part of a team's scratch slot (T / side buffers and, when
+// off-diagonal blocks are not saved, the X / P blocks); the digit planes of the
+// mixed-precision products follow.
+__host__ __device__ inline size_t fp64_slot_bytes(int n, int b, size_t es, bool save) {
+  const size_t bb = (size_t)b * b;
+  size_t s = 4 * bb + invert_side_elems(b);
+  if (!save) s += 2 * (size_t)(n - 1) * bb;
+  return (s * es + 255) / 256 * 256;
+}
 
 // Per-instance meeting point of its team (64 bytes apart).
 struct ItemArea {
@@ -76,13 +92,18 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
   const unsigned flags = hdr->flags;
   const bool save = flags & SINVB_SAVE_OFFDIAG;
   const bool inplace = flags & SINVB_INPLACE;
+  // mixed precision: block products on the int8 tensor cores; this CTA holds
+  // its TMEM for the whole persistent loop
+  const int oz_digits = (std::is_same<T, cplx>::value && (flags & SINVB_PREC_MIXED)) ? mixed_digits(flags) : 0;
+  __shared__ OzState oz_state;
+  if (oz_digits) oz_setup(&oz_state);
   __shared__ int sh_slot;
   while (true) {
     if (threadIdx.x == 0) sh_slot = (int)atomicAdd(&hdr->queue_head, 1u);
     __syncthreads();
     const int s = sh_slot;
     __syncthreads();  // sh_slot is rewritten by the next dequeue
-    if (s >= total_slots) return;
+    if (s >= total_slots) break;
     int lo = 0, hi = count - 1;  // last entry with slot_start <= s
     while (lo < hi) {
       int mid = (lo + hi + 1) >> 1;
@@ -123,6 +144,9 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
     p.flags = flags;
     p.ckpt = nullptr;
     p.ckpt_every = 1;
+    p.oz_digits = oz_digits;
+    p.oz_scratch = slot + fp64_slot_bytes(e.n, e.b, sizeof(T), save);
+    p.oz = &oz_state;
     if (e.b <= 32)
       rgf_sweep<T, 32, 32>(team, p, smem);
     else
@@ -134,6 +158,7 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
       if (st) report(&hdr->status, st);
     }
   }
+  if (oz_digits) oz_teardown(&oz_state);
 }
 
 constexpr size_t kBatchedSmem = sizeof(GjShared<cplx>) > (size_t)gemm_smem_elems<cplx, 64, 64>() * 16
@@ -156,12 +181,12 @@ static BatchLayout batch_layout(const sinvb_batch_desc* d, int count, int dtype,
   BatchLayout L{};
   const size_t es = elem_bytes(dtype);
   const bool save = flags & SINVB_SAVE_OFFDIAG;
+  const bool mixed = flags & SINVB_PREC_MIXED;
   size_t slot = 0;
   for (int k = 0; k < count; k++) {
-    size_t bb = (size_t)d[k].b * d[k].b;
-    size_t s = 4 * bb + invert_side_elems(d[k].b);
-    if (!save) s += 2 * (size_t)(d[k].n - 1) * bb;
-    slot = std::max(slot, s * es);
+    size_t s = fp64_slot_bytes(d[k].n, d[k].b, es, save);
+    if (mixed) s += 2 * oz_op_scratch(d[k].b, d[k].b, d[k].b, mixed_digits(flags));
+    slot = std::max(slot, s);
   }
   L.nslots = batch_slots();
   L.desc_offset = sizeof(WsHeader);
@@ -202,9 +227,11 @@ static int team_size(int b, unsigned flags) {
 }
 
 template <class T>
-static int launch_batched(void* ws, int count, cudaStream_t stream) {
+static int launch_batched(void* ws, int count, unsigned flags, cudaStream_t stream) {
   auto k = rgf_batched_kernel<T>;
-  SINVB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchedSmem));
+  size_t smem = kBatchedSmem;
+  if (flags & SINVB_PREC_MIXED) smem = std::max(smem, oz_smem_bytes(mixed_digits(flags)));
+  SINVB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   // reset status, barrier and queue, and every instance's team area
   SINVB_CUDA(cudaMemsetAsync(ws, 0, 16, stream));
   const size_t items_offset = align_up(sizeof(WsHeader) + (size_t)count * sizeof(BatchEntry<cplx>), 256);
@@ -212,7 +239,7 @@ static int launch_batched(void* ws, int count, cudaStream_t stream) {
   unsigned char* w = (unsigned char*)ws;
   void* args[] = {(void*)&w};
   // cooperative: every CTA resident, so a team member waiting for the others always gets them
-  SINVB_CUDA(cudaLaunchCooperativeKernel((const void*)k, dim3(batch_slots()), dim3(kThreads), args, kBatchedSmem,
+  SINVB_CUDA(cudaLaunchCooperativeKernel((const void*)k, dim3(batch_slots()), dim3(kThreads), args, smem,
                                          stream));
   return SINVB_OK;
 }
@@ -265,21 +292,25 @@ static int upload_and_run(const sinvb_batch_desc* d, int count, unsigned flags, 
   // the pageable copies above are staged before they return; the host arrays may go
   {
     std::lock_guard<std::mutex> lock(g_count_mutex);
-    count_table()[ws] = count;
+    count_table()[ws] = {count, flags};
   }
-  return launch_batched<T>(ws, count, stream);
+  return launch_batched<T>(ws, count, flags, stream);
 }
 
 template <class T>
 static int rerun(void* ws, cudaStream_t stream) {
   int count = -1;
+  unsigned flags = 0;
   {
     std::lock_guard<std::mutex> lock(g_count_mutex);
     auto it = count_table().find(ws);
-    if (it != count_table().end()) count = it->second;
+    if (it != count_table().end()) {
+      count = it->second.first;
+      flags = it->second.second;
+    }
   }
   if (count < 1) return SINVB_EINVAL;  // nothing uploaded into this workspace
-  return launch_batched<T>(ws, count, stream);
+  return launch_batched<T>(ws, count, flags, stream);
 }
 
 }  // namespace sinvb
@@ -295,7 +326,10 @@ size_t sinvb_rgf_batched_workspace_size(const sinvb_batch_desc* descs, int count
 
 int sinvb_rgf_batched_z(const sinvb_batch_desc* descs, int count, unsigned flags, void* workspace,
                         size_t workspace_bytes, int* status, sinvb_stream_t stream) {
-  if (flags & SINVB_PREC_MIXED) return SINVB_EUNSUPPORTED;
+  if ((flags & SINVB_PREC_MIXED) && mixed_digits(flags) > kOzMaxDigits) return SINVB_EINVAL;
+  if (flags & SINVB_PREC_MIXED)
+    for (int k = 0; k < count; k++)
+      if (descs && 2 * descs[k].b > (1 << 14)) return SINVB_EINVAL;
   return upload_and_run<cplx>(descs, count, flags, workspace, workspace_bytes, status, (cudaStream_t)stream,
                               SINVB_C128);
 }

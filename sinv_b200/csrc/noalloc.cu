@@ -118,6 +118,9 @@ extern "C" int sinvb_rgf_z_noalloc(const void* diag, const void* upper, const vo
   p.flags = flags;
   p.ckpt = nullptr;
   p.ckpt_every = 1;
+  p.oz_digits = 0;
+  p.oz_scratch = nullptr;
+  p.oz = nullptr;
   if (b <= 32) return launch_noalloc<32, 32>(p, status, st);
   return launch_noalloc<64, 64>(p, status, st);
 }

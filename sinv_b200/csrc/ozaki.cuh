@@ -96,7 +96,7 @@ __device__ __forceinline__ void oz_store16(int8_t* plane, int r, int k16, int R,
 
 // A side: exponents e_i and digit planes of the embedded rows, work spread over
 // `nthreads_total` threads with global index `gtid` (one warp per complex row).
-__device__ void oz_slice_a(const cplx* A, int lda, const OzShape& s, int8_t* planes, int* ea, int gwarp,
+__device__ inline void oz_slice_a(const cplx* A, int lda, const OzShape& s, int8_t* planes, int* ea, int gwarp,
                            int nwarps) {
   const int lane = threadIdx.x & 31;
   const int K = s.K;
@@ -147,7 +147,7 @@ __device__ void oz_slice_a(const cplx* A, int lda, const OzShape& s, int8_t* pla
 // B side: exponents f_j and digit planes of B^T rows [Re B(:,j) | Im B(:,j)],
 // one thread per (column j, 16-byte K group); column maxima first (one thread
 // per column).
-__device__ void oz_slice_b_exponents(const cplx* B, int ldb, const OzShape& s, int* fb, int gtid, int nthreads) {
+__device__ inline void oz_slice_b_exponents(const cplx* B, int ldb, const OzShape& s, int* fb, int gtid, int nthreads) {
   for (int j = gtid; j < s.N; j += nthreads) {
     double amax = 0.0;
     for (int k = 0; k < s.K; k++) {
@@ -158,7 +158,7 @@ __device__ void oz_slice_b_exponents(const cplx* B, int ldb, const OzShape& s, i
   }
 }
 
-__device__ void oz_slice_b_digits(const cplx* B, int ldb, const OzShape& s, int8_t* planes, const int* fb,
+__device__ inline void oz_slice_b_digits(const cplx* B, int ldb, const OzShape& s, int8_t* planes, const int* fb,
                                   int gtid, int nthreads) {
   const int groups = s.Kp / 16;
   const int K = s.K;
@@ -200,7 +200,7 @@ __host__ __device__ constexpr size_t oz_smem_bytes(int S) {
 }
 
 // One-time set-up by the whole CTA: barriers and a TMEM allocation (warp 0).
-__device__ void oz_setup(OzState* st) {
+__device__ inline void oz_setup(OzState* st) {
   if (threadIdx.x == 0) {
     for (int s = 0; s < kOzStages; s++) {
       mbar_init(&st->full[s], 1);
@@ -217,7 +217,7 @@ __device__ void oz_setup(OzState* st) {
   tc_fence_after();
 }
 
-__device__ void oz_teardown(OzState* st) {
+__device__ inline void oz_teardown(OzState* st) {
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -238,7 +238,7 @@ struct OzOp {
 
 // One 64 x 64 complex output tile on the tensor cores.  Called by all threads
 // of the CTA; returns false when a bounded wait gave up (status reported).
-__device__ bool oz_tile(const OzOp& op, int tm, int tn, OzState* st, unsigned char* smem, int* status) {
+__device__ inline bool oz_tile(const OzOp& op, int tm, int tn, OzState* st, unsigned char* smem, int* status) {
   const OzShape& s = op.s;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nkb = s.Kp / kOzKBlock;
@@ -348,6 +348,72 @@ __device__ bool oz_tile(const OzOp& op, int tm, int tn, OzState* st, unsigned ch
   }
   __syncthreads();
   return ok_flag != 0;
+}
+
+// Scratch one GEMM of the team routine needs: exponents and digit planes.
+__host__ __device__ inline size_t oz_op_scratch(int M, int N, int K, int S) {
+  const OzShape s = oz_shape(M, N, K, S);
+  return (size_t)oz_pad(M * 4, 256) + oz_pad(N * 4, 256) + (size_t)S * (s.a_plane() + s.b_plane());
+}
+
+// Up to 2 independent complex block products C = beta D + alpha A B on the
+// int8 tensor cores, spread over a team of CTAs (the mixed-precision form of
+// team_gemm).  Three phases: digits of every A and exponents of every B;
+// digits of every B; output tiles.  The caller synchronises after the last.
+// Only plain (non-transposed) operands.  Returns false when a wait gave up.
+template <class Team>
+__device__ bool team_gemm_ozaki(Team& team, const GemmOp<cplx>* ops, int nops, int S, unsigned char* scratch,
+                                OzState* st, unsigned char* smem, int* status) {
+  OzOp oz[2];
+  unsigned char* p = scratch;
+  for (int i = 0; i < nops; i++) {
+    const GemmOp<cplx>& g = ops[i];
+    OzOp& o = oz[i];
+    o.s = oz_shape(g.M, g.N, g.K, S);
+    o.ea = reinterpret_cast<int*>(p);
+    p += oz_pad(g.M * 4, 256);
+    o.fb = reinterpret_cast<int*>(p);
+    p += oz_pad(g.N * 4, 256);
+    o.a_planes = reinterpret_cast<int8_t*>(p);
+    p += (size_t)S * o.s.a_plane();
+    o.b_planes = reinterpret_cast<int8_t*>(p);
+    p += (size_t)S * o.s.b_plane();
+    o.D = g.D;
+    o.C = g.C;
+    o.ldd = g.ldd;
+    o.ldc = g.ldc;
+    o.alpha = g.alpha;
+    o.beta = g.beta;
+  }
+  const int warps = blockDim.x >> 5;
+  const int gwarp = team.rank() * warps + (threadIdx.x >> 5), nwarps = team.size() * warps;
+  const int gtid = team.rank() * blockDim.x + threadIdx.x, nthr = team.size() * blockDim.x;
+  for (int i = 0; i < nops; i++) {
+    oz_slice_a(ops[i].A, ops[i].lda, oz[i].s, const_cast<int8_t*>(oz[i].a_planes), const_cast<int*>(oz[i].ea),
+               gwarp, nwarps);
+    oz_slice_b_exponents(ops[i].B, ops[i].ldb, oz[i].s, const_cast<int*>(oz[i].fb), gtid, nthr);
+  }
+  if (!team.sync()) return false;
+  for (int i = 0; i < nops; i++)
+    oz_slice_b_digits(ops[i].B, ops[i].ldb, oz[i].s, const_cast<int8_t*>(oz[i].b_planes), oz[i].fb, gtid, nthr);
+  fence_proxy_async_smem();
+  // digit planes are read by the bulk-copy (async) proxy of other CTAs
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+  if (!team.sync()) return false;
+  // and, on the reading side, after the barrier that made them visible
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+  int counts[2], total = 0;
+  for (int i = 0; i < nops; i++) {
+    counts[i] = (oz_pad(oz[i].s.M, kOzTileM) / kOzTileM) * (oz[i].s.Np / kOzTileN);
+    total += counts[i];
+  }
+  for (int t = team.rank(); t < total; t += team.size()) {
+    int i = 0, local = t;
+    while (local >= counts[i]) local -= counts[i++];
+    const int tn_count = oz[i].s.Np / kOzTileN;
+    if (!oz_tile(oz[i], local / tn_count, local % tn_count, st, smem, status)) return false;
+  }
+  return true;
 }
 
 }  // namespace sinvb

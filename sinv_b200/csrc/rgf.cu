@@ -114,6 +114,9 @@ static int run_rgf(const T* diag, const T* upper, const T* lower, int n, int b, 
   RgfParams<T> p;
   p.ckpt = ckpt;
   p.ckpt_every = ckpt_every;
+  p.oz_digits = 0;
+  p.oz_scratch = nullptr;
+  p.oz = nullptr;
   p.diag = diag;
   p.upper = upper;
   p.lower = lower;
