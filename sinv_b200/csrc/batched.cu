@@ -78,7 +78,7 @@ static_assert(sizeof(ItemArea) == 64, "64-byte item areas");
 // so a team completes as soon as its last member frees up; with teams sized
 // by block size (large blocks first) members mostly arrive together.  Every
 // CTA of the launch is resident (cooperative launch), so each team wait ends.
-template <class T>
+template <class T, bool Mixed>
 __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char* ws) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* smem = reinterpret_cast<T*>(smem_raw);
@@ -94,9 +94,9 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
   const bool inplace = flags & SINVB_INPLACE;
   // mixed precision: block products on the int8 tensor cores; this CTA holds
   // its TMEM for the whole persistent loop
-  const int oz_digits = (std::is_same<T, cplx>::value && (flags & SINVB_PREC_MIXED)) ? mixed_digits(flags) : 0;
+  const int oz_digits = Mixed ? mixed_digits(flags) : 0;
   __shared__ OzState oz_state;
-  if (oz_digits) oz_setup(&oz_state);
+  if (Mixed) oz_setup(&oz_state);
   __shared__ int sh_slot;
   while (true) {
     if (threadIdx.x == 0) sh_slot = (int)atomicAdd(&hdr->queue_head, 1u);
@@ -148,9 +148,9 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
     p.oz_scratch = slot + fp64_slot_bytes(e.n, e.b, sizeof(T), save);
     p.oz = &oz_state;
     if (e.b <= 32)
-      rgf_sweep<T, 32, 32>(team, p, smem);
+      rgf_sweep<T, 32, 32, Mixed>(team, p, smem);
     else
-      rgf_sweep<T, 64, 64>(team, p, smem);
+      rgf_sweep<T, 64, 64, Mixed>(team, p, smem);
     __syncthreads();
     if (rank == 0 && threadIdx.x == 0) {
       int st = *((volatile int*)&item->status);
@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
       if (st) report(&hdr->status, st);
     }
   }
-  if (oz_digits) oz_teardown(&oz_state);
+  if (Mixed) oz_teardown(&oz_state);
 }
 
 constexpr size_t kBatchedSmem = sizeof(GjShared<cplx>) > (size_t)gemm_smem_elems<cplx, 64, 64>() * 16
@@ -228,7 +228,8 @@ static int team_size(int b, unsigned flags) {
 
 template <class T>
 static int launch_batched(void* ws, int count, unsigned flags, cudaStream_t stream) {
-  auto k = rgf_batched_kernel<T>;
+  const bool mixed = std::is_same<T, cplx>::value && (flags & SINVB_PREC_MIXED);
+  auto k = mixed ? rgf_batched_kernel<T, std::is_same<T, cplx>::value> : rgf_batched_kernel<T, false>;
   size_t smem = kBatchedSmem;
   if (flags & SINVB_PREC_MIXED) smem = std::max(smem, oz_smem_bytes(mixed_digits(flags)));
   SINVB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

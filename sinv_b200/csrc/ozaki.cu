@@ -7,47 +7,27 @@
 
 namespace sinvb {
 
-struct OzLayout {
-  size_t ea, fb, ap, bp, total;
-};
-
-static OzLayout oz_layout(const OzShape& s) {
-  OzLayout L{};
-  size_t off = sizeof(WsHeader);
-  auto take = [&](size_t bytes) {
-    size_t at = off;
-    off += align_up(bytes, 256);
-    return at;
-  };
-  L.ea = take((size_t)s.M * 4);
-  L.fb = take((size_t)s.N * 4);
-  L.ap = take((size_t)s.S * s.a_plane());
-  L.bp = take((size_t)s.S * s.b_plane());
-  L.total = off;
-  return L;
-}
+// Workspace: the status header, then the exponents and digit planes in the
+// order oz_bind lays them out.
+static size_t oz_workspace_bytes(int M, int N, int K, int S) { return sizeof(WsHeader) + oz_op_scratch(M, N, K, S); }
 
 __global__ void __launch_bounds__(256) oz_slice_a_kernel(const cplx* A, int lda, OzShape s, int8_t* planes, int* ea) {
   const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
   oz_slice_a(A, lda, s, planes, ea, gwarp, nwarps);
 }
-__global__ void __launch_bounds__(256) oz_slice_bexp_kernel(const cplx* B, int ldb, OzShape s, int* fb) {
-  oz_slice_b_exponents(B, ldb, s, fb, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
-}
-__global__ void __launch_bounds__(256) oz_slice_bdig_kernel(const cplx* B, int ldb, OzShape s, int8_t* planes,
-                                                            const int* fb) {
-  oz_slice_b_digits(B, ldb, s, planes, fb, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+// one CTA per 32-column block of B
+__global__ void __launch_bounds__(256) oz_slice_b_kernel(const cplx* B, int ldb, OzShape s, int8_t* planes, int* fb) {
+  __shared__ double red[256];
+  oz_slice_b_block(B, ldb, s, planes, fb, blockIdx.x, red);
 }
 
-// Persistent over output tiles: every CTA allocates TMEM once and walks tiles.
+// Persistent over output tiles: every CTA allocates TMEM once and walks tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ...
 __global__ void __launch_bounds__(256, 1) oz_gemm_kernel(OzOp op, int* status) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ OzState st;
   oz_setup(&st);
-  const int tiles_m = oz_pad(op.s.M, kOzTileM) / kOzTileM, tiles_n = op.s.Np / kOzTileN;
-  for (int t = blockIdx.x; t < tiles_m * tiles_n; t += gridDim.x) {
-    if (!oz_tile(op, t / tiles_n, t % tiles_n, &st, smem, status)) break;
-  }
+  oz_tiles(&op, 1, blockIdx.x, gridDim.x, &st, smem, status);
   oz_teardown(&st);
 }
 
@@ -59,7 +39,7 @@ extern "C" {
 
 size_t sinvb_zgemm_ozaki_workspace_size(int M, int N, int K, int digits) {
   if (M < 1 || N < 1 || K < 1 || digits < 1 || digits > kOzMaxDigits) return 0;
-  return oz_layout(oz_shape(M, N, K, digits)).total;
+  return oz_workspace_bytes(M, N, K, digits);
 }
 
 int sinvb_zgemm_ozaki(int M, int N, int K, double alpha, const void* A, int lda, const void* B, int ldb,
@@ -71,35 +51,24 @@ int sinvb_zgemm_ozaki(int M, int N, int K, double alpha, const void* A, int lda,
   for (const void* q : {A, B, D, (const void*)C})
     if (q && (uintptr_t)q % 16) return SINVB_EINVAL;
   if ((uintptr_t)workspace % 256) return SINVB_EWORKSPACE;
-  const OzShape s = oz_shape(M, N, K, digits);
-  const OzLayout L = oz_layout(s);
-  if (workspace_bytes < L.total) return SINVB_EWORKSPACE;
+  if (workspace_bytes < oz_workspace_bytes(M, N, K, digits)) return SINVB_EWORKSPACE;
   int rc = check_device();
   if (rc) return rc;
   unsigned char* ws = (unsigned char*)workspace;
   cudaStream_t st = (cudaStream_t)stream;
   SINVB_CUDA(cudaMemsetAsync(ws, 0, sizeof(WsHeader), st));
   const int sms = device_sm_count();
-  oz_slice_a_kernel<<<sms * 4, 256, 0, st>>>((const cplx*)A, lda, s, (int8_t*)(ws + L.ap), (int*)(ws + L.ea));
-  oz_slice_bexp_kernel<<<(N + 255) / 256, 256, 0, st>>>((const cplx*)B, ldb, s, (int*)(ws + L.fb));
-  oz_slice_bdig_kernel<<<sms * 4, 256, 0, st>>>((const cplx*)B, ldb, s, (int8_t*)(ws + L.bp),
-                                                (const int*)(ws + L.fb));
-  SINVB_CUDA(cudaGetLastError());
   OzOp op;
-  op.a_planes = (const int8_t*)(ws + L.ap);
-  op.b_planes = (const int8_t*)(ws + L.bp);
-  op.ea = (const int*)(ws + L.ea);
-  op.fb = (const int*)(ws + L.fb);
-  op.s = s;
-  op.D = (const cplx*)D;
-  op.C = (cplx*)C;
-  op.ldd = ldd;
-  op.ldc = ldc;
-  op.alpha = alpha;
-  op.beta = beta;
+  oz_bind(op, M, N, K, digits, ws + sizeof(WsHeader), alpha, beta, (const cplx*)D, ldd, (cplx*)C, ldc);
+  const int ctas_a = (M + 7) / 8;  // one warp per row, 8 warps per CTA
+  oz_slice_a_kernel<<<ctas_a < sms * 4 ? ctas_a : sms * 4, 256, 0, st>>>(
+      (const cplx*)A, lda, op.s, const_cast<int8_t*>(op.a_planes), const_cast<int*>(op.ea));
+  oz_slice_b_kernel<<<(N + 31) / 32, 256, 0, st>>>((const cplx*)B, ldb, op.s, const_cast<int8_t*>(op.b_planes),
+                                                   const_cast<int*>(op.fb));
+  SINVB_CUDA(cudaGetLastError());
   const size_t smem = oz_smem_bytes(digits);
   SINVB_CUDA(cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int tiles = (oz_pad(M, kOzTileM) / kOzTileM) * (s.Np / kOzTileN);
+  const int tiles = op.tiles;
   const int grid = tiles < sms ? tiles : sms;
   oz_gemm_kernel<<<grid, 256, smem, st>>>(op, &((WsHeader*)ws)->status);
   SINVB_CUDA(cudaGetLastError());

@@ -9,24 +9,29 @@
 //
 // Splitting.  Every row i of A is scaled by 2^-e_i (e_i: exponent of the row's
 // largest |Re| or |Im|) and every column j of B by 2^-f_j, so all entries lie
-// in (-1, 1).  Each scaled value x is cut into S signed 7-bit digits
-//   x = sum_t d_t 2^(-6-7(t-1)),  d_t in [-64, 64]  (the first digit carries 6 bits)
-// which int8 holds exactly.  Digit products are exact in int32 and so are their
-// sums (|sum| <= S * 2K * 64 * 64 < 2^31 for 2K <= 2^14), so the only error is
-// the truncation after S digits: levels L = s + t <= S + 1 are kept,
-//   C_ij = 2^(e_i + f_j) sum_L 2^(-12-7(L-2)) sum_{s+t=L} (A_s B_t)_ij.
+// in (-1, 1).  Each scaled value x is rounded once to a multiple of 2^(1-7S)
+// and cut into S signed digits
+//   x = sum_t d_t 2^(-6-7(t-1)),  t = 1..S,  d_1 in [-64, 64], d_t in [-64, 63]
+// which int8 holds exactly.  Digit products are exact in int32 and so are
+// their sums (|sum| <= S * 2K * 2^12 < 2^31 for 2K <= 2^16), so the only
+// errors are the rounding of the operands and the levels L = s + t > S + 1
+// left out:
+//   C_ij = 2^(e_i + f_j) sum_{L=2}^{S+1} 2^(-12-7(L-2)) sum_{s+t=L} (A_s B_t)_ij.
 // Complex operands are embedded as real matrices: per 64-row group of A the
 // 128 MMA rows are [Re A | -Im A] (64 rows) and [Im A | Re A] (64 rows), B^T
 // rows are [Re B(:,j) | Im B(:,j)], so one 128 x 64 x 2K real product gives the
 // real and the imaginary parts of a 64 x 64 complex tile in TMEM lanes 0-63 and
-// 64-127, and one accumulator of 64 columns holds a level (S levels <= 512
-// columns).
+// 64-127.  Each level owns 64 TMEM columns (S <= 8 levels in 512 columns);
+// the B digits of one A digit s sit next to each other in shared memory, so a
+// single MMA with N = 64 * (number of B digits, at most 4) feeds the run of
+// levels s+1, s+2, ... at once.
 //
 // Digit planes live in global memory in the canonical K-major core-matrix
-// layout of tcgen05 (8 rows x 16 bytes per core matrix): the 64-byte K-block of
-// 128 A rows (or 64 B rows) is one contiguous 8 KB (4 KB) run that a single
-// bulk copy moves into shared memory.
-//   offset(r, k) = ((k/64 * R/8 + r/8) * 4 + (k%64)/16) * 128 + (r%8) * 16 + k%16
+// layout of tcgen05 (8 rows x 16 bytes per core matrix) with 32-byte K-blocks:
+// the K-block of 128 A rows (64 B rows) is one contiguous 4 KB (2 KB) run that
+// one bulk copy moves into the shared-memory stage ring.
+//   offset(r, k) = ((k/32 * R/8 + r/8) * 2 + (k%32)/16) * 128 + (r%8) * 16 + k%16
+// The two halves of K' = 2 Kh start at 0 and Kh = K rounded up to 16.
 #pragma once
 
 #include "block_gemm.cuh"
@@ -35,20 +40,26 @@
 namespace sinvb {
 
 constexpr int kOzMaxDigits = 8;
-constexpr int kOzTileM = 64;   // complex rows per tile (128 MMA rows)
-constexpr int kOzTileN = 64;   // complex columns per tile
-constexpr int kOzKBlock = 64;  // bytes of K per pipeline stage
-constexpr int kOzStages = 2;
+constexpr int kOzTileM = 64;                          // complex rows per output tile (128 MMA rows)
+constexpr int kOzTileN = 64;                          // complex columns per output tile
+constexpr int kOzKBlock = 32;                         // K' bytes per pipeline stage (one MMA's K)
+constexpr int kOzMaxStages = 4;
+constexpr int kOzStageA = 2 * kOzTileM * kOzKBlock;   // 4096 B: one digit of a 128-row A block
+constexpr int kOzStageB = kOzTileN * kOzKBlock;       // 2048 B: one digit of a 64-row B^T block
+constexpr int kOzEpiCols = 32;                        // output columns per epilogue staging pass
+constexpr int kOzEpiStride = 2 * kOzEpiCols + 1;      // doubles per staged row (odd: no bank conflicts)
+constexpr size_t kOzEpiBytes = (size_t)kOzTileM * kOzEpiStride * 8;
 
 __host__ __device__ inline int oz_pad(int x, int m) { return (x + m - 1) / m * m; }
 
 // Geometry of the digit planes of one operand pair.
 struct OzShape {
-  int M, N, K;   // complex sizes
-  int Mp;        // A-embed rows (multiple of 128)
-  int Np;        // B^T rows (multiple of 64)
-  int Kp;        // bytes of K' = 2K, multiple of 64
-  int S;         // digits
+  int M, N, K;  // complex sizes
+  int Kh;       // K rounded up to 16: start of the second half of K'
+  int Mp;       // embedded A rows: 2 x (M rounded up to 64)
+  int Np;       // B^T rows: N rounded up to 64
+  int Kp;       // K' = 2 Kh bytes per digit row (a multiple of 32)
+  int S;        // digits
   __host__ __device__ size_t a_plane() const { return (size_t)Mp * Kp; }
   __host__ __device__ size_t b_plane() const { return (size_t)Np * Kp; }
 };
@@ -56,29 +67,41 @@ struct OzShape {
 __host__ __device__ inline OzShape oz_shape(int M, int N, int K, int S) {
   OzShape s;
   s.M = M; s.N = N; s.K = K; s.S = S;
+  s.Kh = oz_pad(K, 16);
   s.Mp = oz_pad(M, kOzTileM) * 2;
   s.Np = oz_pad(N, kOzTileN);
-  s.Kp = oz_pad(2 * K, kOzKBlock);
+  s.Kp = 2 * s.Kh;
   return s;
 }
 
-__device__ __forceinline__ size_t oz_off(int r, int k, int R) {
-  return ((size_t)((k >> 6) * (R >> 3) + (r >> 3)) * 4 + ((k & 63) >> 4)) * 128 + (r & 7) * 16 + (k & 15);
+// Stages of the ring: four, three for 8 digits (shared memory).
+__host__ __device__ constexpr int oz_stages(int S) { return S <= 7 ? 4 : 3; }
+__host__ __device__ constexpr size_t oz_stage_bytes(int S) { return (size_t)S * (kOzStageA + kOzStageB); }
+// ring, epilogue staging, 128 exponents of the tile being written
+__host__ __device__ constexpr size_t oz_smem_bytes(int S) {
+  return oz_stages(S) * oz_stage_bytes(S) + kOzEpiBytes + 128 * sizeof(int);
 }
 
-// Digits of x in (-1, 1): d[0] has 6 bits, the rest 7.
-__device__ __forceinline__ void oz_digits(double x, int S, int (&d)[kOzMaxDigits]) {
-  double v = x * 64.0;
+__host__ __device__ __forceinline__ size_t oz_off(int r, int k, int R) {
+  return ((size_t)((k >> 5) * (R >> 3) + (r >> 3)) * 2 + ((k >> 4) & 1)) * 128 + (r & 7) * 16 + (k & 15);
+}
+
+// The S digits of x in (-1, 1), most significant first (d[0] .. d[S-1]):
+// m = round(x 2^(7S-1)) cut into base-128 digits with balanced remainders
+// from the bottom up.
+__device__ __forceinline__ void oz_split(double x, int S, double scale, int (&d)[kOzMaxDigits]) {
+  long long m = __double2ll_rn(x * scale);
 #pragma unroll
-  for (int t = 0; t < kOzMaxDigits; t++) {
+  for (int t = kOzMaxDigits - 1; t >= 1; t--) {
     if (t < S) {
-      double r = rint(v);
-      d[t] = (int)r;
-      v = (v - r) * 128.0;
+      const int r = (int)((m + 64) & 127) - 64;
+      d[t] = r;
+      m = (m - r) >> 7;
     } else {
       d[t] = 0;
     }
   }
+  d[0] = (int)m;
 }
 
 __device__ __forceinline__ int oz_exponent(double amax) {
@@ -87,128 +110,206 @@ __device__ __forceinline__ int oz_exponent(double amax) {
   return e;
 }
 
-// Writes 16 consecutive K bytes of one digit-plane row.
-__device__ __forceinline__ void oz_store16(int8_t* plane, int r, int k16, int R, const int8_t (&v)[16]) {
-  int4 w;
-  memcpy(&w, v, 16);
-  *reinterpret_cast<int4*>(plane + oz_off(r, k16, R)) = w;
+__device__ __forceinline__ double oz_pow2(int e) {
+  return (e >= -1022 && e <= 1023) ? __longlong_as_double((long long)(e + 1023) << 52) : ldexp(1.0, e);
 }
 
-// A side: exponents e_i and digit planes of the embedded rows, work spread over
-// `nthreads_total` threads with global index `gtid` (one warp per complex row).
+__device__ __forceinline__ uint32_t oz_byte(int d, int q) { return (uint32_t)(uint8_t)(int8_t)d << (8 * q); }
+
+// Writes the digits of 4 consecutive K (Re x[q], Im y[q]) of one complex row
+// of A into both embedded rows.
+__device__ __forceinline__ void oz_store_a4(int8_t* planes, const OzShape& s, int rre, int k4, const double (&x)[4],
+                                            const double (&y)[4], double scale) {
+  uint32_t wr[kOzMaxDigits], wi[kOzMaxDigits], wn[kOzMaxDigits];
+#pragma unroll
+  for (int t = 0; t < kOzMaxDigits; t++) wr[t] = wi[t] = wn[t] = 0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    int dx[kOzMaxDigits], dy[kOzMaxDigits];
+    oz_split(x[q], s.S, scale, dx);
+    oz_split(y[q], s.S, scale, dy);
+#pragma unroll
+    for (int t = 0; t < kOzMaxDigits; t++) {
+      wr[t] |= oz_byte(dx[t], q);
+      wi[t] |= oz_byte(dy[t], q);
+      wn[t] |= oz_byte(-dy[t], q);
+    }
+  }
+  const int rim = rre + kOzTileM;
+#pragma unroll
+  for (int t = 0; t < kOzMaxDigits; t++) {
+    if (t < s.S) {
+      int8_t* pl = planes + (size_t)t * s.a_plane();
+      *reinterpret_cast<uint32_t*>(pl + oz_off(rre, k4, s.Mp)) = wr[t];         // [Re A | -Im A]
+      *reinterpret_cast<uint32_t*>(pl + oz_off(rre, s.Kh + k4, s.Mp)) = wn[t];
+      *reinterpret_cast<uint32_t*>(pl + oz_off(rim, k4, s.Mp)) = wi[t];         // [Im A |  Re A]
+      *reinterpret_cast<uint32_t*>(pl + oz_off(rim, s.Kh + k4, s.Mp)) = wr[t];
+    }
+  }
+}
+
+// A side: exponents e_i and the digit planes of the embedded rows.  One warp
+// per complex row (warp `gwarp` of `nwarps`); lane l takes K = 4l + 128m + q
+// (q < 4), so every load of the warp is one contiguous 2 KB run.  Rows of up to
+// kOzRowRegs x 128 entries are read once and held in registers; longer rows
+// are read a second time for the digits.  Rows past M are left unwritten: they
+// only reach output rows that are never stored.
+constexpr int kOzRowRegs = 4;
 __device__ inline void oz_slice_a(const cplx* A, int lda, const OzShape& s, int8_t* planes, int* ea, int gwarp,
-                           int nwarps) {
+                                  int nwarps) {
   const int lane = threadIdx.x & 31;
-  const int K = s.K;
-  for (int i = gwarp; i < s.Mp / 2; i += nwarps) {
-    const int rre = (i / kOzTileM) * 2 * kOzTileM + (i % kOzTileM), rim = rre + kOzTileM;
+  const double scale = (double)(1ull << (7 * s.S - 1));
+  const int chunks = (s.Kh + 127) / 128;
+  for (int i = gwarp; i < s.M; i += nwarps) {
+    const cplx* row = A + (size_t)i * lda;
+    cplx v[kOzRowRegs][4];
     double amax = 0.0;
-    if (i < s.M)
-      for (int k = lane; k < K; k += 32) {
-        cplx v = A[(size_t)i * lda + k];
-        amax = fmax(amax, fmax(fabs(v.re), fabs(v.im)));
+#pragma unroll
+    for (int m = 0; m < kOzRowRegs; m++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int k = 128 * m + 4 * lane + q;
+        v[m][q] = (m < chunks && k < s.K) ? row[k] : cplx{0.0, 0.0};
+        amax = fmax(amax, fmax(fabs(v[m][q].re), fabs(v[m][q].im)));
+      }
+    for (int m = kOzRowRegs; m < chunks; m++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int k = 128 * m + 4 * lane + q;
+        if (k < s.K) {
+          const cplx w = row[k];
+          amax = fmax(amax, fmax(fabs(w.re), fabs(w.im)));
+        }
       }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
     const int e = oz_exponent(amax);
-    if (lane == 0 && i < s.M) ea[i] = e;
+    if (lane == 0) ea[i] = e;
     const double sc = ldexp(1.0, -e);
-    // each lane: one 16-byte group of K' for both embedded rows, all planes
-    for (int k16 = lane * 16; k16 < s.Kp; k16 += 32 * 16) {
-      int8_t re_row[kOzMaxDigits][16], im_row[kOzMaxDigits][16];
+    const int rre = (i / kOzTileM) * 2 * kOzTileM + i % kOzTileM;
 #pragma unroll
-      for (int q = 0; q < 16; q++) {
-        const int kk = k16 + q;
-        int dx[kOzMaxDigits], dy[kOzMaxDigits];
-        const int k = kk < K ? kk : kk - K;
-        double x = 0.0, y = 0.0;
-        if (i < s.M && kk < 2 * K) {
-          cplx v = A[(size_t)i * lda + k];
-          x = v.re * sc;
-          y = v.im * sc;
-        }
-        oz_digits(x, s.S, dx);
-        oz_digits(y, s.S, dy);
-        const bool first = kk < K;
+    for (int m = 0; m < kOzRowRegs; m++) {
+      const int k4 = 128 * m + 4 * lane;
+      if (m < chunks && k4 < s.Kh) {
+        double x[4], y[4];
 #pragma unroll
-        for (int t = 0; t < kOzMaxDigits; t++) {
-          re_row[t][q] = (int8_t)(first ? dx[t] : -dy[t]);  // [Re A | -Im A]
-          im_row[t][q] = (int8_t)(first ? dy[t] : dx[t]);   // [Im A |  Re A]
+        for (int q = 0; q < 4; q++) {
+          x[q] = v[m][q].re * sc;
+          y[q] = v[m][q].im * sc;
         }
+        oz_store_a4(planes, s, rre, k4, x, y, scale);
       }
-      for (int t = 0; t < s.S; t++) {
-        oz_store16(planes + t * s.a_plane(), rre, k16, s.Mp, re_row[t]);
-        oz_store16(planes + t * s.a_plane(), rim, k16, s.Mp, im_row[t]);
+    }
+    for (int m = kOzRowRegs; m < chunks; m++) {
+      const int k4 = 128 * m + 4 * lane;
+      if (k4 < s.Kh) {
+        double x[4], y[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int k = k4 + q;
+          const cplx w = k < s.K ? row[k] : cplx{0.0, 0.0};
+          x[q] = w.re * sc;
+          y[q] = w.im * sc;
+        }
+        oz_store_a4(planes, s, rre, k4, x, y, scale);
       }
     }
   }
 }
 
-// B side: exponents f_j and digit planes of B^T rows [Re B(:,j) | Im B(:,j)],
-// one thread per (column j, 16-byte K group); column maxima first (one thread
-// per column).
-__device__ inline void oz_slice_b_exponents(const cplx* B, int ldb, const OzShape& s, int* fb, int gtid, int nthreads) {
-  for (int j = gtid; j < s.N; j += nthreads) {
-    double amax = 0.0;
-    for (int k = 0; k < s.K; k++) {
-      cplx v = B[(size_t)k * ldb + j];
+// B side for the 32 columns [32 cb, 32 cb + 32): column exponents f_j (warps
+// split the rows, lanes are columns, then a reduction in shared memory), then
+// the digit planes of the B^T rows [Re B(:,j) | Im B(:,j)] (each thread 16
+// consecutive K of one column, one 16-byte store per digit and half).  Called
+// by every thread of the CTA; `red` is blockDim.x doubles of shared memory.
+// Columns past N are left unwritten (they only reach discarded outputs).
+__device__ inline void oz_slice_b_block(const cplx* B, int ldb, const OzShape& s, int8_t* planes, int* fb, int cb,
+                                        double* red) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int j = cb * 32 + lane;
+  const bool valid = j < s.N;
+  double amax = 0.0;
+  if (valid) {
+#pragma unroll 8
+    for (int k = warp; k < s.K; k += nw) {
+      const cplx v = B[(size_t)k * ldb + j];
       amax = fmax(amax, fmax(fabs(v.re), fabs(v.im)));
     }
-    fb[j] = oz_exponent(amax);
   }
-}
-
-__device__ inline void oz_slice_b_digits(const cplx* B, int ldb, const OzShape& s, int8_t* planes, const int* fb,
-                                  int gtid, int nthreads) {
-  const int groups = s.Kp / 16;
-  const int K = s.K;
-  for (int w = gtid; w < s.Np * groups; w += nthreads) {
-    const int j = w % s.Np, k16 = (w / s.Np) * 16;  // consecutive threads: consecutive columns (coalesced reads)
-    const double sc = j < s.N ? ldexp(1.0, -fb[j]) : 0.0;
-    int8_t row[kOzMaxDigits][16];
+  red[warp * 32 + lane] = amax;
+  __syncthreads();
+  if (warp == 0) {
+    for (int w = 1; w < nw; w++) amax = fmax(amax, red[w * 32 + lane]);
+    const int f = oz_exponent(amax);
+    if (valid) fb[j] = f;
+    red[lane] = ldexp(1.0, -f);
+  }
+  __syncthreads();
+  const double sc = red[lane];
+  const double scale = (double)(1ull << (7 * s.S - 1));
+  for (int k16 = 16 * warp; k16 < s.Kh; k16 += 16 * nw) {
+    uint32_t wr[kOzMaxDigits][4], wi[kOzMaxDigits][4];
+#pragma unroll
+    for (int t = 0; t < kOzMaxDigits; t++)
+#pragma unroll
+      for (int w = 0; w < 4; w++) wr[t][w] = wi[t][w] = 0;
 #pragma unroll
     for (int q = 0; q < 16; q++) {
-      const int kk = k16 + q;
-      double x = 0.0;
-      if (j < s.N && kk < 2 * K) {
-        cplx v = B[(size_t)(kk < K ? kk : kk - K) * ldb + j];
-        x = (kk < K ? v.re : v.im) * sc;
+      const int k = k16 + q;
+      double x = 0.0, y = 0.0;
+      if (valid && k < s.K) {
+        const cplx v = B[(size_t)k * ldb + j];
+        x = v.re * sc;
+        y = v.im * sc;
       }
-      int d[kOzMaxDigits];
-      oz_digits(x, s.S, d);
+      int dx[kOzMaxDigits], dy[kOzMaxDigits];
+      oz_split(x, s.S, scale, dx);
+      oz_split(y, s.S, scale, dy);
 #pragma unroll
-      for (int t = 0; t < kOzMaxDigits; t++) row[t][q] = (int8_t)d[t];
+      for (int t = 0; t < kOzMaxDigits; t++) {
+        wr[t][q >> 2] |= oz_byte(dx[t], q & 3);
+        wi[t][q >> 2] |= oz_byte(dy[t], q & 3);
+      }
     }
-    for (int t = 0; t < s.S; t++) oz_store16(planes + t * s.b_plane(), j, k16, s.Np, row[t]);
+    if (valid) {
+#pragma unroll
+      for (int t = 0; t < kOzMaxDigits; t++) {
+        if (t < s.S) {
+          int8_t* pl = planes + (size_t)t * s.b_plane();
+          *reinterpret_cast<uint4*>(pl + oz_off(j, k16, s.Np)) = make_uint4(wr[t][0], wr[t][1], wr[t][2], wr[t][3]);
+          *reinterpret_cast<uint4*>(pl + oz_off(j, s.Kh + k16, s.Np)) =
+              make_uint4(wi[t][0], wi[t][1], wi[t][2], wi[t][3]);
+        }
+      }
+    }
   }
+  __syncthreads();  // `red` is reused by the next column block
 }
 
-// Shared state of the tile routine; lives in shared memory for the whole kernel.
+// Per-CTA state of the tile pipeline; lives in shared memory for the whole kernel.
 struct OzState {
-  uint64_t full[kOzStages];
-  uint64_t empty[kOzStages];
-  uint64_t done;
-  unsigned tmem;       // TMEM base address
-  unsigned kblocks;    // k-blocks streamed so far (stage / phase bookkeeping)
-  unsigned tiles;      // tiles finished so far (phase of `done`)
+  uint64_t full[kOzMaxStages];   // stage filled (bulk copies landed)
+  uint64_t empty[kOzMaxStages];  // stage consumed (MMAs done)
+  uint64_t tmem_full;            // a tile's accumulators are complete
+  uint64_t tmem_empty;           // the epilogue has read them (128 arrivals)
+  unsigned tmem;                 // TMEM base address
+  unsigned kblocks;              // k-blocks streamed so far (stage index and phases of full / empty)
+  unsigned tiles;                // tiles finished so far (phases of tmem_full / tmem_empty)
+  int fail;                      // a bounded wait gave up: the pipeline phases are no longer known
 };
-
-__host__ __device__ constexpr size_t oz_stage_bytes(int S) { return (size_t)S * (128 + 64) * kOzKBlock; }
-__host__ __device__ constexpr size_t oz_smem_bytes(int S) {
-  return kOzStages * oz_stage_bytes(S) > (size_t)kOzTileM * kOzTileN * 16 ? kOzStages * oz_stage_bytes(S)
-                                                                          : (size_t)kOzTileM * kOzTileN * 16;
-}
 
 // One-time set-up by the whole CTA: barriers and a TMEM allocation (warp 0).
 __device__ inline void oz_setup(OzState* st) {
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kOzStages; s++) {
+    for (int s = 0; s < kOzMaxStages; s++) {
       mbar_init(&st->full[s], 1);
       mbar_init(&st->empty[s], 1);
     }
-    mbar_init(&st->done, 1);
+    mbar_init(&st->tmem_full, 1);
+    mbar_init(&st->tmem_empty, 128);
     st->kblocks = 0;
     st->tiles = 0;
+    st->fail = 0;
     mbar_fence_init();
   }
   if ((threadIdx.x >> 5) == 0) tmem_alloc(&st->tmem, 512);
@@ -224,196 +325,302 @@ __device__ inline void oz_teardown(OzState* st) {
   if ((threadIdx.x >> 5) == 0) tmem_dealloc(st->tmem, 512);
 }
 
+// One product of a tile routine call: digit planes, exponents, output.
 struct OzOp {
   const int8_t* a_planes;
   const int8_t* b_planes;
   const int* ea;
   const int* fb;
   OzShape s;
+  int tiles;  // (Mp / 128) x (Np / 64) output tiles, numbered row by row
   const cplx* D;
   cplx* C;
   int ldd, ldc;
   double alpha, beta;
 };
 
-// One 64 x 64 complex output tile on the tensor cores.  Called by all threads
-// of the CTA; returns false when a bounded wait gave up (status reported).
-__device__ inline bool oz_tile(const OzOp& op, int tm, int tn, OzState* st, unsigned char* smem, int* status) {
-  const OzShape& s = op.s;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nkb = s.Kp / kOzKBlock;
-  const unsigned kb0 = st->kblocks;
-  const size_t stage = oz_stage_bytes(s.S);
-  __shared__ int ok_flag;
-  if (threadIdx.x == 0) ok_flag = 1;
-  __syncthreads();
-  if (warp == 0 && lane == 0) {  // producer: bulk copies of the digit tiles
-    for (int kb = 0; kb < nkb; kb++) {
-      const unsigned g = kb0 + kb, sidx = g % kOzStages, use = g / kOzStages;
-      if (use > 0 && !mbar_wait(&st->empty[sidx], (use - 1) & 1, status)) { ok_flag = 0; break; }
-      unsigned char* base = smem + sidx * stage;
-      mbar_expect_tx(&st->full[sidx], (unsigned)stage);
-      const size_t aoff = (size_t)(kb * (s.Mp >> 3) + (tm * 2 * kOzTileM >> 3)) * 512;
-      const size_t boff = (size_t)(kb * (s.Np >> 3) + (tn * kOzTileN >> 3)) * 512;
-      for (int t = 0; t < s.S; t++) {
-        bulk_g2s(base + t * 8192, op.a_planes + t * s.a_plane() + aoff, 8192, &st->full[sidx]);
-        bulk_g2s(base + s.S * 8192 + t * 4096, op.b_planes + t * s.b_plane() + boff, 4096, &st->full[sidx]);
-      }
+__host__ __device__ inline int oz_tile_count(const OzShape& s) { return (s.Mp / (2 * kOzTileM)) * (s.Np / kOzTileN); }
+
+// The MMAs of one k-block: for every A digit a, B digits 1 .. S+1-a in runs
+// of at most 4 (N <= 256); the run starting at B digit b0 lands in the TMEM
+// columns of levels a+b0, a+b0+1, ...  The A digit 1 runs cover every level,
+// so on the first k-block of a tile they overwrite the accumulators.
+template <int S>
+__device__ __forceinline__ void oz_issue_s(uint64_t adesc, uint64_t bdesc, unsigned tmem, bool first) {
+#pragma unroll
+  for (int a = 1; a <= S; a++) {
+#pragma unroll
+    for (int b0 = 1; b0 <= S + 1 - a; b0 += 4) {
+      const int cnt = (S + 2 - a - b0) < 4 ? (S + 2 - a - b0) : 4;
+      mma_i8(tmem + (unsigned)((a + b0 - 2) * 64), adesc + (uint64_t)((a - 1) * (kOzStageA >> 4)),
+             bdesc + (uint64_t)((b0 - 1) * (kOzStageB >> 4)), idesc_i8(128, 64 * cnt), !(first && a == 1));
     }
-  } else if (warp == 1 && lane == 0) {  // MMA issuer
-    const uint32_t idesc = idesc_i8(128, 64);
-    bool good = true;
-    for (int kb = 0; kb < nkb && good; kb++) {
-      const unsigned g = kb0 + kb, sidx = g % kOzStages, use = g / kOzStages;
-      if (!mbar_wait(&st->full[sidx], use & 1, status)) { good = false; break; }
-      tc_fence_after();
-      unsigned char* base = smem + sidx * stage;
-      for (int L = 2; L <= s.S + 1; L++) {
-        const unsigned dcol = st->tmem + (L - 2) * 64;
-        for (int a = 1; a < L; a++) {
-          const int b = L - a;
-          if (a > s.S || b > s.S) continue;
-          for (int ks = 0; ks < 2; ks++) {
-            const uint64_t ad = sdesc(base + (a - 1) * 8192 + ks * 256, 128, 512);
-            const uint64_t bd = sdesc(base + s.S * 8192 + (b - 1) * 4096 + ks * 256, 128, 512);
-            const bool first = kb == 0 && a == (L - s.S > 1 ? L - s.S : 1) && ks == 0;
-            mma_i8(dcol, ad, bd, idesc, !first);
+  }
+}
+
+__device__ __forceinline__ void oz_issue(int S, uint64_t adesc, uint64_t bdesc, unsigned tmem, bool first) {
+  switch (S) {
+    case 1: oz_issue_s<1>(adesc, bdesc, tmem, first); break;
+    case 2: oz_issue_s<2>(adesc, bdesc, tmem, first); break;
+    case 3: oz_issue_s<3>(adesc, bdesc, tmem, first); break;
+    case 4: oz_issue_s<4>(adesc, bdesc, tmem, first); break;
+    case 5: oz_issue_s<5>(adesc, bdesc, tmem, first); break;
+    case 6: oz_issue_s<6>(adesc, bdesc, tmem, first); break;
+    case 7: oz_issue_s<7>(adesc, bdesc, tmem, first); break;
+    default: oz_issue_s<8>(adesc, bdesc, tmem, first); break;
+  }
+}
+
+// Barrier 1 of the four epilogue warps (128 threads), and its AND-reduction.
+__device__ __forceinline__ void oz_epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+__device__ __forceinline__ bool oz_epi_all(bool p) {
+  int r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.b32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, 1, 128, p;\n\t"
+      "selp.b32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((int)p)
+      : "memory");
+  return r != 0;
+}
+
+struct OzTileRef {
+  int op, tm, tn;
+};
+__device__ __forceinline__ OzTileRef oz_tile_ref(const OzOp* ops, int nops, int t) {
+  int i = 0;
+  while (i + 1 < nops && t >= ops[i].tiles) t -= ops[i].tiles, i++;
+  const int tn_count = ops[i].s.Np / kOzTileN;
+  return {i, t / tn_count, t % tn_count};
+}
+
+// Output tiles t = first, first + stride, ... of the ops (numbered op by op):
+// warp 0 streams digit blocks into the stage ring, warp 1 issues the MMAs into
+// TMEM, warps 4-7 read the levels back, rebuild FP64 and write C, while the
+// MMAs of the next tile already run.  Called by every thread of the CTA with
+// the same arguments; all ops have the same digit count.  Returns false when
+// a bounded wait gave up (status reported).
+__device__ inline bool oz_tiles(const OzOp* ops, int nops, int first, int stride, OzState* st, unsigned char* smem,
+                                int* status) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = ops[0].s.S, NS = oz_stages(S);
+  const size_t stage = oz_stage_bytes(S);
+  int total = 0;
+  for (int i = 0; i < nops; i++) total += ops[i].tiles;
+  unsigned my_kb = 0, my_tiles = 0;
+  for (int t = first; t < total; t += stride) {
+    my_kb += ops[oz_tile_ref(ops, nops, t).op].s.Kp / kOzKBlock;
+    my_tiles++;
+  }
+  // the ring area may hold data written through the generic proxy (FP64 tiles)
+  fence_proxy_async_smem();
+  __syncthreads();
+  const unsigned kb0 = st->kblocks, t0 = st->tiles;
+  if (st->fail) return false;
+
+  if (warp == 0) {
+    if (lane == 0) {  // producer
+      unsigned g = kb0;
+      bool ok = true;
+      for (int t = first; t < total && ok; t += stride) {
+        const OzTileRef r = oz_tile_ref(ops, nops, t);
+        const OzOp& op = ops[r.op];
+        const int nkb = op.s.Kp / kOzKBlock;
+        for (int kb = 0; kb < nkb; kb++, g++) {
+          const unsigned sidx = g % NS, use = g / NS;
+          if (use > 0 && !mbar_wait(&st->empty[sidx], (use - 1) & 1, status)) {
+            ok = false;
+            break;
+          }
+          unsigned char* base = smem + sidx * stage;
+          mbar_expect_tx(&st->full[sidx], (unsigned)stage);
+          const size_t aoff = (size_t)(kb * (op.s.Mp >> 3) + r.tm * 16) * 256;
+          const size_t boff = (size_t)(kb * (op.s.Np >> 3) + r.tn * 8) * 256;
+          for (int d = 0; d < S; d++) {
+            bulk_g2s(base + d * kOzStageA, op.a_planes + d * op.s.a_plane() + aoff, kOzStageA, &st->full[sidx]);
+            bulk_g2s(base + S * kOzStageA + d * kOzStageB, op.b_planes + d * op.s.b_plane() + boff, kOzStageB,
+                     &st->full[sidx]);
           }
         }
       }
-      mma_commit(&st->empty[sidx]);
+      if (!ok) st->fail = 1;
     }
-    if (good) mma_commit(&st->done);
-    else ok_flag = 0;
-  }
-  // epilogue: TMEM lanes -> FP64, staged in shared memory as a 64 x 64 complex tile
-  __syncthreads();
-  const bool ok = ok_flag != 0;
-  double* ctile = reinterpret_cast<double*>(smem);  // [64][64] complex as interleaved doubles
-  if (warp >= 4) {
-    bool good = ok && mbar_wait(&st->done, st->tiles & 1, status);
-    if (!good) ok_flag = 0;
-    tc_fence_after();
-    // wait for the producer's last copies too: all MMAs done implies all stages consumed
-    const int q = warp - 4;
-    const int r = 32 * q + lane;               // MMA row in the tile
-    const int i = r & 63, part = r >> 6;       // complex row, 0 = Re, 1 = Im
-    double acc[64];
-#pragma unroll
-    for (int c = 0; c < 64; c++) acc[c] = 0.0;
-    if (good) {
-      for (int L = 2; L <= s.S + 1; L++) {
-        const double scale = ldexp(1.0, -12 - 7 * (L - 2));
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      unsigned g = kb0, T = t0;
+      bool ok = true;
+      const uint64_t d0 = sdesc(smem, 128, 256);
+      for (int t = first; t < total && ok; t += stride) {
+        const OzOp& op = ops[oz_tile_ref(ops, nops, t).op];
+        const int nkb = op.s.Kp / kOzKBlock;
+        if (T > 0 && !mbar_wait(&st->tmem_empty, (T - 1) & 1, status)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        for (int kb = 0; kb < nkb; kb++, g++) {
+          const unsigned sidx = g % NS, use = g / NS;
+          if (!mbar_wait(&st->full[sidx], use & 1, status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint64_t ad = d0 + (uint64_t)((sidx * stage) >> 4);
+          oz_issue(S, ad, ad + (uint64_t)((S * kOzStageA) >> 4), st->tmem, kb == 0);
+          mma_commit(&st->empty[sidx]);
+        }
+        if (!ok) break;
+        mma_commit(&st->tmem_full);
+        T++;
+      }
+      if (!ok) st->fail = 1;
+    }
+  } else if (warp >= 4) {  // epilogue: TMEM lanes 32 (warp - 4) ...
+    const int et = threadIdx.x - 128;       // 0..127
+    const int i = et & 63, part = et >> 6;  // complex row in the tile, 0 = Re / 1 = Im
+    const unsigned lane_base = st->tmem + ((unsigned)(32 * (warp - 4)) << 16);
+    double* stg = reinterpret_cast<double*>(smem + NS * stage);
+    int* exps = reinterpret_cast<int*>(smem + NS * stage + kOzEpiBytes);  // [0,64): f_j, [64,128): e_i
+    unsigned T = t0;
+    bool ok = true;
+    for (int t = first; t < total; t += stride) {
+      const OzTileRef r = oz_tile_ref(ops, nops, t);
+      const OzOp& op = ops[r.op];
+      {  // exponents of the tile's columns and rows, fetched while the MMAs run
+        const int g = et < 64 ? r.tn * kOzTileN + et : r.tm * kOzTileM + (et - 64);
+        exps[et] = et < 64 ? (g < op.s.N ? op.fb[g] : 0) : (g < op.s.M ? op.ea[g] : 0);
+      }
+      ok = oz_epi_all(mbar_wait(&st->tmem_full, T & 1, status));  // also orders `exps`
+      if (!ok) break;
+      tc_fence_after();
+      // Horner over the levels, least significant first: acc = sum_L v_L 2^(-7(L-2))
+      double acc[2 * kOzEpiCols];
+      {
+        int v[32];
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-          int v[32];
-          tmem_ld32(st->tmem + ((unsigned)(32 * q) << 16) + (L - 2) * 64 + h * 32, v);
+          tmem_ld32(lane_base + (unsigned)((S - 1) * 64 + h * 32), v);
           tmem_wait_ld();
 #pragma unroll
-          for (int c = 0; c < 32; c++) acc[h * 32 + c] = fma((double)v[c], scale, acc[h * 32 + c]);
+          for (int c = 0; c < 32; c++) acc[h * 32 + c] = (double)v[c];
         }
-      }
-    }
-    tc_fence_before();
-    const int gi = tm * kOzTileM + i;
-    const int ei = (gi < s.M) ? op.ea[gi] : 0;
+        for (int L = S; L >= 2; L--) {
 #pragma unroll
-    for (int c = 0; c < 64; c++) {
-      const int gj = tn * kOzTileN + c;
-      const int fj = (gj < s.N) ? op.fb[gj] : 0;
-      ctile[(i * 64 + c) * 2 + part] = ldexp(acc[c], ei + fj);
-    }
-  }
-  __syncthreads();
-  // coalesced write of the tile: C = beta D + alpha * product
-  if (ok_flag) {
-    for (int e = threadIdx.x; e < kOzTileM * kOzTileN; e += blockDim.x) {
-      const int i = e / kOzTileN, c = e % kOzTileN;
-      const int gi = tm * kOzTileM + i, gj = tn * kOzTileN + c;
-      if (gi < s.M && gj < s.N) {
-        cplx v{op.alpha * ctile[e * 2], op.alpha * ctile[e * 2 + 1]};
-        if (op.D) {
-          cplx d = op.D[(size_t)gi * op.ldd + gj];
-          v = cplx{fma(op.beta, d.re, v.re), fma(op.beta, d.im, v.im)};
+          for (int h = 0; h < 2; h++) {
+            tmem_ld32(lane_base + (unsigned)((L - 2) * 64 + h * 32), v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < 32; c++) acc[h * 32 + c] = fma(acc[h * 32 + c], 0.0078125, (double)v[c]);
+          }
         }
-        op.C[(size_t)gi * op.ldc + gj] = v;
       }
+      tc_fence_before();
+      mbar_arrive(&st->tmem_empty);  // the next tile's MMAs may overwrite the accumulators
+      const int ei = exps[64 + i] - 12;
+      const bool addend = op.D != nullptr && op.beta != 0.0;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+#pragma unroll
+        for (int c = 0; c < kOzEpiCols; c++)
+          stg[i * kOzEpiStride + 2 * c + part] =
+              op.alpha * acc[h * kOzEpiCols + c] * oz_pow2(ei + exps[h * kOzEpiCols + c]);
+        oz_epi_sync();
+        // 16 entries per thread: all addend loads first, then the stores
+        constexpr int kPer = kOzTileM * kOzEpiCols / 128;
+        cplx dv[kPer];
+#pragma unroll
+        for (int m = 0; m < kPer; m++) {
+          const int e = et + 128 * m, ii = e / kOzEpiCols, c = e % kOzEpiCols;
+          const int gi = r.tm * kOzTileM + ii, gj = r.tn * kOzTileN + h * kOzEpiCols + c;
+          dv[m] = (addend && gi < op.s.M && gj < op.s.N) ? op.D[(size_t)gi * op.ldd + gj] : cplx{0.0, 0.0};
+        }
+#pragma unroll
+        for (int m = 0; m < kPer; m++) {
+          const int e = et + 128 * m, ii = e / kOzEpiCols, c = e % kOzEpiCols;
+          const int gi = r.tm * kOzTileM + ii, gj = r.tn * kOzTileN + h * kOzEpiCols + c;
+          if (gi < op.s.M && gj < op.s.N) {
+            const double re = stg[ii * kOzEpiStride + 2 * c], im = stg[ii * kOzEpiStride + 2 * c + 1];
+            op.C[(size_t)gi * op.ldc + gj] = addend ? cplx{fma(op.beta, dv[m].re, re), fma(op.beta, dv[m].im, im)}
+                                                    : cplx{re, im};
+          }
+        }
+        oz_epi_sync();
+      }
+      T++;
     }
-  }
-  fence_proxy_async_smem();  // generic smem writes before the next tile's bulk copies
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    st->kblocks = kb0 + nkb;
-    st->tiles += 1;
+    if (!ok && et == 0) st->fail = 1;
   }
   __syncthreads();
-  return ok_flag != 0;
+  if (threadIdx.x == 0 && !st->fail) {
+    st->kblocks = kb0 + my_kb;
+    st->tiles = t0 + my_tiles;
+  }
+  __syncthreads();
+  return st->fail == 0;
 }
 
-// Scratch one GEMM of the team routine needs: exponents and digit planes.
+// Scratch one product of the team routine needs: exponents and digit planes.
 __host__ __device__ inline size_t oz_op_scratch(int M, int N, int K, int S) {
   const OzShape s = oz_shape(M, N, K, S);
   return (size_t)oz_pad(M * 4, 256) + oz_pad(N * 4, 256) + (size_t)S * (s.a_plane() + s.b_plane());
 }
 
+// Fills an OzOp for C = beta D + alpha A B with its scratch at `p`; returns the
+// end of the scratch it took.
+__host__ __device__ inline unsigned char* oz_bind(OzOp& o, int M, int N, int K, int S, unsigned char* p, double alpha,
+                                                  double beta, const cplx* D, int ldd, cplx* C, int ldc) {
+  o.s = oz_shape(M, N, K, S);
+  o.tiles = oz_tile_count(o.s);
+  o.ea = reinterpret_cast<int*>(p);
+  p += oz_pad(M * 4, 256);
+  o.fb = reinterpret_cast<int*>(p);
+  p += oz_pad(N * 4, 256);
+  o.a_planes = reinterpret_cast<int8_t*>(p);
+  p += (size_t)S * o.s.a_plane();
+  o.b_planes = reinterpret_cast<int8_t*>(p);
+  p += (size_t)S * o.s.b_plane();
+  o.D = D;
+  o.C = C;
+  o.ldd = ldd;
+  o.ldc = ldc;
+  o.alpha = alpha;
+  o.beta = beta;
+  return p;
+}
+
 // Up to 2 independent complex block products C = beta D + alpha A B on the
 // int8 tensor cores, spread over a team of CTAs (the mixed-precision form of
-// team_gemm).  Three phases: digits of every A and exponents of every B;
-// digits of every B; output tiles.  The caller synchronises after the last.
-// Only plain (non-transposed) operands.  Returns false when a wait gave up.
+// team_gemm).  Two phases: digits and exponents of every operand (A rows over
+// all warps of the team, B column blocks over its CTAs), then the output tiles
+// (over its CTAs).  The caller synchronises after the second.  Plain
+// (non-transposed) operands only.  Returns false when a wait gave up.
 template <class Team>
 __device__ bool team_gemm_ozaki(Team& team, const GemmOp<cplx>* ops, int nops, int S, unsigned char* scratch,
                                 OzState* st, unsigned char* smem, int* status) {
+  if (st->fail) return false;
   OzOp oz[2];
   unsigned char* p = scratch;
   for (int i = 0; i < nops; i++) {
     const GemmOp<cplx>& g = ops[i];
-    OzOp& o = oz[i];
-    o.s = oz_shape(g.M, g.N, g.K, S);
-    o.ea = reinterpret_cast<int*>(p);
-    p += oz_pad(g.M * 4, 256);
-    o.fb = reinterpret_cast<int*>(p);
-    p += oz_pad(g.N * 4, 256);
-    o.a_planes = reinterpret_cast<int8_t*>(p);
-    p += (size_t)S * o.s.a_plane();
-    o.b_planes = reinterpret_cast<int8_t*>(p);
-    p += (size_t)S * o.s.b_plane();
-    o.D = g.D;
-    o.C = g.C;
-    o.ldd = g.ldd;
-    o.ldc = g.ldc;
-    o.alpha = g.alpha;
-    o.beta = g.beta;
+    p = oz_bind(oz[i], g.M, g.N, g.K, S, p, g.alpha, g.beta, g.D, g.ldd, g.C, g.ldc);
   }
   const int warps = blockDim.x >> 5;
   const int gwarp = team.rank() * warps + (threadIdx.x >> 5), nwarps = team.size() * warps;
-  const int gtid = team.rank() * blockDim.x + threadIdx.x, nthr = team.size() * blockDim.x;
+  double* red = reinterpret_cast<double*>(smem);
   for (int i = 0; i < nops; i++) {
     oz_slice_a(ops[i].A, ops[i].lda, oz[i].s, const_cast<int8_t*>(oz[i].a_planes), const_cast<int*>(oz[i].ea),
                gwarp, nwarps);
-    oz_slice_b_exponents(ops[i].B, ops[i].ldb, oz[i].s, const_cast<int*>(oz[i].fb), gtid, nthr);
+    for (int cb = team.rank(); cb < (ops[i].N + 31) / 32; cb += team.size())
+      oz_slice_b_block(ops[i].B, ops[i].ldb, oz[i].s, const_cast<int8_t*>(oz[i].b_planes),
+                       const_cast<int*>(oz[i].fb), cb, red);
   }
-  if (!team.sync()) return false;
-  for (int i = 0; i < nops; i++)
-    oz_slice_b_digits(ops[i].B, ops[i].ldb, oz[i].s, const_cast<int8_t*>(oz[i].b_planes), oz[i].fb, gtid, nthr);
-  fence_proxy_async_smem();
-  // digit planes are read by the bulk-copy (async) proxy of other CTAs
+  // the planes are read by the bulk-copy (async) proxy of every CTA of the team
   asm volatile("fence.proxy.async.global;" ::: "memory");
   if (!team.sync()) return false;
-  // and, on the reading side, after the barrier that made them visible
   asm volatile("fence.proxy.async.global;" ::: "memory");
-  int counts[2], total = 0;
-  for (int i = 0; i < nops; i++) {
-    counts[i] = (oz_pad(oz[i].s.M, kOzTileM) / kOzTileM) * (oz[i].s.Np / kOzTileN);
-    total += counts[i];
-  }
-  for (int t = team.rank(); t < total; t += team.size()) {
-    int i = 0, local = t;
-    while (local >= counts[i]) local -= counts[i++];
-    const int tn_count = oz[i].s.Np / kOzTileN;
-    if (!oz_tile(oz[i], local / tn_count, local % tn_count, st, smem, status)) return false;
-  }
-  return true;
+  return oz_tiles(oz, nops, team.rank(), team.size(), st, smem, status);
 }
 
 }  // namespace sinvb

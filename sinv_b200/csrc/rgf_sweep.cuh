@@ -58,26 +58,27 @@ struct RgfParams {
   T* ckpt;         // optional: g_{s*c-1} saved to ckpt[s-1] (s = 1, 2, ...) for the adjoint
   int ckpt_every;  // c
   // mixed precision (complex only): block products on the int8 tensor cores
-  int oz_digits;              // 0: every product in FP64 (DMMA)
+  int oz_digits;              // digits of the tensor-core products (used by Mixed sweeps only)
   unsigned char* oz_scratch;  // 2 x oz_op_scratch(b, b, b, digits) bytes
   OzState* oz;                // per-CTA pipeline state (TMEM allocated by the kernel)
 };
 
-// The block products of a sweep phase: FP64 DMMA, or the int8 tensor-core
-// Ozaki products when the sweep runs in mixed precision.  The block inverses
-// always stay in FP64.
-template <class T, int BM, int BN, class Team>
+// The block products of a sweep phase: FP64 DMMA, or (Mixed, complex only)
+// the int8 tensor-core Ozaki products with p.oz_digits (>= 1) digits.  The
+// block inverses always stay in FP64.  Mixed is a template switch so that
+// kernels without the tensor-core path do not carry its registers.
+template <class T, int BM, int BN, bool Mixed, class Team>
 __device__ __forceinline__ bool sweep_gemm(Team& team, const RgfParams<T>& p, const GemmOp<T>* ops, int nops, T* smem) {
-  if constexpr (std::is_same<T, cplx>::value) {
-    if (p.oz_digits > 0)
-      return team_gemm_ozaki(team, ops, nops, p.oz_digits, p.oz_scratch, p.oz,
-                             reinterpret_cast<unsigned char*>(smem), p.status);
+  if constexpr (Mixed && std::is_same<T, cplx>::value) {
+    return team_gemm_ozaki(team, ops, nops, p.oz_digits, p.oz_scratch, p.oz, reinterpret_cast<unsigned char*>(smem),
+                           p.status);
+  } else {
+    team_gemm<T, BM, BN>(team, ops, nops, smem);
+    return true;
   }
-  team_gemm<T, BM, BN>(team, ops, nops, smem);
-  return true;
 }
 
-template <class T, int BM, int BN, class Team>
+template <class T, int BM, int BN, bool Mixed = false, class Team>
 __device__ void rgf_sweep(Team& team, const RgfParams<T>& p, T* smem) {
   const int n = p.n, b = p.b;
   const size_t bb = (size_t)b * b;
@@ -104,7 +105,7 @@ __device__ void rgf_sweep(Team& team, const RgfParams<T>& p, T* smem) {
       GemmOp<T> ops[2];
       ops[0] = make_op<T>(b, b, b, 1.0, g, b, U, b, nullptr, 0, Xd, b);
       ops[1] = make_op<T>(b, b, b, 1.0, L, b, g, b, nullptr, 0, Pd, b);
-      if (!sweep_gemm<T, BM, BN>(team, p, ops, 2, smem)) return;
+      if (!sweep_gemm<T, BM, BN, Mixed>(team, p, ops, 2, smem)) return;
       if (inplace && i >= 2)  // P_{i-1} over A_{i-2,i-1}, dead since F2 of step i-1
         team_copy<T>(team, b, b, (i & 1) ? p.T1 : p.T3, b, p.Gu + (i - 2) * bb, b);
       if (p.ckpt && i % p.ckpt_every == 0)  // checkpoint g_{i-1} for the adjoint
@@ -113,7 +114,7 @@ __device__ void rgf_sweep(Team& team, const RgfParams<T>& p, T* smem) {
     if (!team.sync()) return;
     {  // F2: S_i = A_ii - P_i U_{i-1}
       GemmOp<T> op = make_op<T>(b, b, b, -1.0, Pd, b, U, b, p.diag + i * bb, b, p.Gd + i * bb, b);
-      if (!sweep_gemm<T, BM, BN>(team, p, &op, 1, smem)) return;
+      if (!sweep_gemm<T, BM, BN, Mixed>(team, p, &op, 1, smem)) return;
       if (inplace)  // X_{i-1} over A_{i,i-1}, dead since F1
         team_copy<T>(team, b, b, Xd, b, p.Gl + (i - 1) * bb, b);
     }
@@ -131,7 +132,7 @@ __device__ void rgf_sweep(Team& team, const RgfParams<T>& p, T* smem) {
     T* Tcur = (i & 1) ? p.T1 : p.T0;
     {  // B1: T = -G_{i+1} P_{i+1}; flush the previous T into G_lower / G_upper
       GemmOp<T> op = make_op<T>(b, b, b, -1.0, p.Gd + (i + 1) * bb, b, p.P + i * bb, b, nullptr, 0, Tcur, b);
-      if (!sweep_gemm<T, BM, BN>(team, p, &op, 1, smem)) return;
+      if (!sweep_gemm<T, BM, BN, Mixed>(team, p, &op, 1, smem)) return;
       if (prevT && save) {
         team_copy<T>(team, b, b, prevT, b, p.Gl + prevI * bb, b);
         if (sym) team_copy<T>(team, b, b, prevT, b, p.Gu + prevI * bb, b, true);
@@ -146,7 +147,7 @@ __device__ void rgf_sweep(Team& team, const RgfParams<T>& p, T* smem) {
         ops[q++] = make_op<T>(b, b, b, -1.0, X, b, p.Gd + (i + 1) * bb, b, nullptr, 0, p.Gu + i * bb, b);
       T* Gii = p.Gd + i * bb;
       ops[q++] = make_op<T>(b, b, b, -1.0, X, b, Tcur, b, Gii, b, Gii, b);
-      if (!sweep_gemm<T, BM, BN>(team, p, ops, q, smem)) return;
+      if (!sweep_gemm<T, BM, BN, Mixed>(team, p, ops, q, smem)) return;
     }
     if (!team.sync()) return;
     prevT = Tcur;
