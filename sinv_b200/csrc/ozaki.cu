@@ -11,14 +11,16 @@ namespace sinvb {
 // order oz_bind lays them out.
 static size_t oz_workspace_bytes(int M, int N, int K, int S) { return sizeof(WsHeader) + oz_op_scratch(M, N, K, S); }
 
-__global__ void __launch_bounds__(256) oz_slice_a_kernel(const cplx* A, int lda, OzShape s, int8_t* planes, int* ea) {
-  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
-  oz_slice_a(A, lda, s, planes, ea, gwarp, nwarps);
-}
-// one CTA per 32-column block of B
-__global__ void __launch_bounds__(256) oz_slice_b_kernel(const cplx* B, int ldb, OzShape s, int8_t* planes, int* fb) {
+// Digits of both operands: CTAs [0, ctas_a) take A rows (one warp per row),
+// the rest one 32-column block of B each.
+__global__ void __launch_bounds__(256) oz_slice_kernel(GemmOp<cplx> g, OzOp op, int ctas_a) {
   __shared__ double red[256];
-  oz_slice_b_block(B, ldb, s, planes, fb, blockIdx.x, red);
+  if ((int)blockIdx.x < ctas_a) {
+    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (ctas_a * blockDim.x) >> 5;
+    oz_slice_ops(op.s.S, &g, &op, 1, gwarp, nwarps, 1 << 30, 1, red);  // A only
+  } else {
+    oz_slice_ops(op.s.S, &g, &op, 1, 1 << 30, 1, blockIdx.x - ctas_a, 1 << 30, red);  // one B block
+  }
 }
 
 // Persistent over output tiles: every CTA allocates TMEM once and walks tiles
@@ -60,11 +62,11 @@ int sinvb_zgemm_ozaki(int M, int N, int K, double alpha, const void* A, int lda,
   const int sms = device_sm_count();
   OzOp op;
   oz_bind(op, M, N, K, digits, ws + sizeof(WsHeader), alpha, beta, (const cplx*)D, ldd, (cplx*)C, ldc);
-  const int ctas_a = (M + 7) / 8;  // one warp per row, 8 warps per CTA
-  oz_slice_a_kernel<<<ctas_a < sms * 4 ? ctas_a : sms * 4, 256, 0, st>>>(
-      (const cplx*)A, lda, op.s, const_cast<int8_t*>(op.a_planes), const_cast<int*>(op.ea));
-  oz_slice_b_kernel<<<(N + 31) / 32, 256, 0, st>>>((const cplx*)B, ldb, op.s, const_cast<int8_t*>(op.b_planes),
-                                                   const_cast<int*>(op.fb));
+  int ctas_a = (M + 7) / 8;  // one warp per row, 8 warps per CTA
+  if (ctas_a > sms * 4) ctas_a = sms * 4;
+  const GemmOp<cplx> g = make_op<cplx>(M, N, K, alpha, (const cplx*)A, lda, (const cplx*)B, ldb, (const cplx*)D, ldd,
+                                       (cplx*)C, ldc);
+  oz_slice_kernel<<<ctas_a + (N + 31) / 32, 256, 0, st>>>(g, op, ctas_a);
   SINVB_CUDA(cudaGetLastError());
   const size_t smem = oz_smem_bytes(digits);
   SINVB_CUDA(cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

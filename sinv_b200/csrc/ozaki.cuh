@@ -86,22 +86,36 @@ __host__ __device__ __forceinline__ size_t oz_off(int r, int k, int R) {
   return ((size_t)((k >> 5) * (R >> 3) + (r >> 3)) * 2 + ((k >> 4) & 1)) * 128 + (r & 7) * 16 + (k & 15);
 }
 
-// The S digits of x in (-1, 1), most significant first (d[0] .. d[S-1]):
-// m = round(x 2^(7S-1)) cut into base-128 digits with balanced remainders
-// from the bottom up.
-__device__ __forceinline__ void oz_split(double x, int S, double scale, int (&d)[kOzMaxDigits]) {
-  long long m = __double2ll_rn(x * scale);
+// The S digits of x in (-1, 1), d[0] most significant: m = round(x 2^(7S-1))
+// cut into base-128 digits with balanced remainders (in [-64, 63]) from the
+// bottom up.  m is split in FP64 as H 2^(7L) + Lo (L = S/2 low digits,
+// |Lo| <= 2^(7L-1)) so the digit arithmetic runs on 32-bit integers; the
+// representation is unique, so the split changes no digit.
+template <int S>
+__device__ __forceinline__ void oz_split(double x, int (&d)[S]) {
+  constexpr int L = S / 2;
+  if constexpr (L == 0) {
+    d[0] = __double2int_rn(x * 64.0);
+  } else {
+    const double m = rint(x * (double)(1ull << (7 * S - 1)));
+    const double h = rint(m * (1.0 / (double)(1ull << (7 * L))));
+    int lo = __double2int_rn(fma(-h, (double)(1ull << (7 * L)), m));
+    int hi = __double2int_rn(h);
 #pragma unroll
-  for (int t = kOzMaxDigits - 1; t >= 1; t--) {
-    if (t < S) {
-      const int r = (int)((m + 64) & 127) - 64;
+    for (int t = S - 1; t >= S - L; t--) {
+      const int r = ((lo + 64) & 127) - 64;
       d[t] = r;
-      m = (m - r) >> 7;
-    } else {
-      d[t] = 0;
+      lo = (lo - r) >> 7;
     }
+    hi += lo;  // carry out of the low part: -1, 0 or 1
+#pragma unroll
+    for (int t = S - L - 1; t >= 1; t--) {
+      const int r = ((hi + 64) & 127) - 64;
+      d[t] = r;
+      hi = (hi - r) >> 7;
+    }
+    d[0] = hi;
   }
-  d[0] = (int)m;
 }
 
 __device__ __forceinline__ int oz_exponent(double amax) {
@@ -114,37 +128,35 @@ __device__ __forceinline__ double oz_pow2(int e) {
   return (e >= -1022 && e <= 1023) ? __longlong_as_double((long long)(e + 1023) << 52) : ldexp(1.0, e);
 }
 
-__device__ __forceinline__ uint32_t oz_byte(int d, int q) { return (uint32_t)(uint8_t)(int8_t)d << (8 * q); }
+// Four signed bytes (low byte of each argument) packed little-endian.
+__device__ __forceinline__ uint32_t oz_pack4(int b0, int b1, int b2, int b3) {
+  return __byte_perm(__byte_perm(b0, b1, 0x0040), __byte_perm(b2, b3, 0x0040), 0x5410);
+}
 
 // Writes the digits of 4 consecutive K (Re x[q], Im y[q]) of one complex row
 // of A into both embedded rows.
+template <int S>
 __device__ __forceinline__ void oz_store_a4(int8_t* planes, const OzShape& s, int rre, int k4, const double (&x)[4],
-                                            const double (&y)[4], double scale) {
-  uint32_t wr[kOzMaxDigits], wi[kOzMaxDigits], wn[kOzMaxDigits];
-#pragma unroll
-  for (int t = 0; t < kOzMaxDigits; t++) wr[t] = wi[t] = wn[t] = 0;
+                                            const double (&y)[4]) {
+  int dx[4][S], dy[4][S];
 #pragma unroll
   for (int q = 0; q < 4; q++) {
-    int dx[kOzMaxDigits], dy[kOzMaxDigits];
-    oz_split(x[q], s.S, scale, dx);
-    oz_split(y[q], s.S, scale, dy);
-#pragma unroll
-    for (int t = 0; t < kOzMaxDigits; t++) {
-      wr[t] |= oz_byte(dx[t], q);
-      wi[t] |= oz_byte(dy[t], q);
-      wn[t] |= oz_byte(-dy[t], q);
-    }
+    oz_split<S>(x[q], dx[q]);
+    oz_split<S>(y[q], dy[q]);
   }
   const int rim = rre + kOzTileM;
+  const size_t o_rr = oz_off(rre, k4, s.Mp), o_rn = oz_off(rre, s.Kh + k4, s.Mp);
+  const size_t o_ir = oz_off(rim, k4, s.Mp), o_in = oz_off(rim, s.Kh + k4, s.Mp);
 #pragma unroll
-  for (int t = 0; t < kOzMaxDigits; t++) {
-    if (t < s.S) {
-      int8_t* pl = planes + (size_t)t * s.a_plane();
-      *reinterpret_cast<uint32_t*>(pl + oz_off(rre, k4, s.Mp)) = wr[t];         // [Re A | -Im A]
-      *reinterpret_cast<uint32_t*>(pl + oz_off(rre, s.Kh + k4, s.Mp)) = wn[t];
-      *reinterpret_cast<uint32_t*>(pl + oz_off(rim, k4, s.Mp)) = wi[t];         // [Im A |  Re A]
-      *reinterpret_cast<uint32_t*>(pl + oz_off(rim, s.Kh + k4, s.Mp)) = wr[t];
-    }
+  for (int t = 0; t < S; t++) {
+    const uint32_t wr = oz_pack4(dx[0][t], dx[1][t], dx[2][t], dx[3][t]);
+    const uint32_t wi = oz_pack4(dy[0][t], dy[1][t], dy[2][t], dy[3][t]);
+    const uint32_t wn = __vsub4(0u, wi);  // bytewise -Im
+    int8_t* pl = planes + (size_t)t * s.a_plane();
+    *reinterpret_cast<uint32_t*>(pl + o_rr) = wr;  // [Re A | -Im A]
+    *reinterpret_cast<uint32_t*>(pl + o_rn) = wn;
+    *reinterpret_cast<uint32_t*>(pl + o_ir) = wi;  // [Im A |  Re A]
+    *reinterpret_cast<uint32_t*>(pl + o_in) = wr;
   }
 }
 
@@ -155,10 +167,10 @@ __device__ __forceinline__ void oz_store_a4(int8_t* planes, const OzShape& s, in
 // are read a second time for the digits.  Rows past M are left unwritten: they
 // only reach output rows that are never stored.
 constexpr int kOzRowRegs = 4;
+template <int S>
 __device__ inline void oz_slice_a(const cplx* A, int lda, const OzShape& s, int8_t* planes, int* ea, int gwarp,
                                   int nwarps) {
   const int lane = threadIdx.x & 31;
-  const double scale = (double)(1ull << (7 * s.S - 1));
   const int chunks = (s.Kh + 127) / 128;
   for (int i = gwarp; i < s.M; i += nwarps) {
     const cplx* row = A + (size_t)i * lda;
@@ -197,7 +209,7 @@ __device__ inline void oz_slice_a(const cplx* A, int lda, const OzShape& s, int8
           x[q] = v[m][q].re * sc;
           y[q] = v[m][q].im * sc;
         }
-        oz_store_a4(planes, s, rre, k4, x, y, scale);
+        oz_store_a4<S>(planes, s, rre, k4, x, y);
       }
     }
     for (int m = kOzRowRegs; m < chunks; m++) {
@@ -211,7 +223,7 @@ __device__ inline void oz_slice_a(const cplx* A, int lda, const OzShape& s, int8
           x[q] = w.re * sc;
           y[q] = w.im * sc;
         }
-        oz_store_a4(planes, s, rre, k4, x, y, scale);
+        oz_store_a4<S>(planes, s, rre, k4, x, y);
       }
     }
   }
@@ -223,6 +235,7 @@ __device__ inline void oz_slice_a(const cplx* A, int lda, const OzShape& s, int8
 // consecutive K of one column, one 16-byte store per digit and half).  Called
 // by every thread of the CTA; `red` is blockDim.x doubles of shared memory.
 // Columns past N are left unwritten (they only reach discarded outputs).
+template <int S>
 __device__ inline void oz_slice_b_block(const cplx* B, int ldb, const OzShape& s, int8_t* planes, int* fb, int cb,
                                         double* red) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -246,40 +259,35 @@ __device__ inline void oz_slice_b_block(const cplx* B, int ldb, const OzShape& s
   }
   __syncthreads();
   const double sc = red[lane];
-  const double scale = (double)(1ull << (7 * s.S - 1));
   for (int k16 = 16 * warp; k16 < s.Kh; k16 += 16 * nw) {
-    uint32_t wr[kOzMaxDigits][4], wi[kOzMaxDigits][4];
-#pragma unroll
-    for (int t = 0; t < kOzMaxDigits; t++)
-#pragma unroll
-      for (int w = 0; w < 4; w++) wr[t][w] = wi[t][w] = 0;
+    cplx v[16];
 #pragma unroll
     for (int q = 0; q < 16; q++) {
       const int k = k16 + q;
-      double x = 0.0, y = 0.0;
-      if (valid && k < s.K) {
-        const cplx v = B[(size_t)k * ldb + j];
-        x = v.re * sc;
-        y = v.im * sc;
-      }
-      int dx[kOzMaxDigits], dy[kOzMaxDigits];
-      oz_split(x, s.S, scale, dx);
-      oz_split(y, s.S, scale, dy);
-#pragma unroll
-      for (int t = 0; t < kOzMaxDigits; t++) {
-        wr[t][q >> 2] |= oz_byte(dx[t], q & 3);
-        wi[t][q >> 2] |= oz_byte(dy[t], q & 3);
-      }
+      v[q] = (valid && k < s.K) ? B[(size_t)k * ldb + j] : cplx{0.0, 0.0};
     }
     if (valid) {
+      uint32_t wr[S][4], wi[S][4];
 #pragma unroll
-      for (int t = 0; t < kOzMaxDigits; t++) {
-        if (t < s.S) {
-          int8_t* pl = planes + (size_t)t * s.b_plane();
-          *reinterpret_cast<uint4*>(pl + oz_off(j, k16, s.Np)) = make_uint4(wr[t][0], wr[t][1], wr[t][2], wr[t][3]);
-          *reinterpret_cast<uint4*>(pl + oz_off(j, s.Kh + k16, s.Np)) =
-              make_uint4(wi[t][0], wi[t][1], wi[t][2], wi[t][3]);
+      for (int g = 0; g < 4; g++) {
+        int dx[4][S], dy[4][S];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          oz_split<S>(v[4 * g + q].re * sc, dx[q]);
+          oz_split<S>(v[4 * g + q].im * sc, dy[q]);
         }
+#pragma unroll
+        for (int t = 0; t < S; t++) {
+          wr[t][g] = oz_pack4(dx[0][t], dx[1][t], dx[2][t], dx[3][t]);
+          wi[t][g] = oz_pack4(dy[0][t], dy[1][t], dy[2][t], dy[3][t]);
+        }
+      }
+      const size_t o_r = oz_off(j, k16, s.Np), o_i = oz_off(j, s.Kh + k16, s.Np);
+#pragma unroll
+      for (int t = 0; t < S; t++) {
+        int8_t* pl = planes + (size_t)t * s.b_plane();
+        *reinterpret_cast<uint4*>(pl + o_r) = make_uint4(wr[t][0], wr[t][1], wr[t][2], wr[t][3]);
+        *reinterpret_cast<uint4*>(pl + o_i) = make_uint4(wi[t][0], wi[t][1], wi[t][2], wi[t][3]);
       }
     }
   }
@@ -590,6 +598,35 @@ __host__ __device__ inline unsigned char* oz_bind(OzOp& o, int M, int N, int K, 
   return p;
 }
 
+// Digits and exponents of the operands of `nops` products: A rows over warp
+// `gwarp` of `nwarps`, B column blocks cb0, cb0 + cbstep, ... (every thread of
+// a CTA calls this with the same cb0 / cbstep).
+template <int S>
+__device__ inline void oz_slice_ops_s(const GemmOp<cplx>* ops, const OzOp* oz, int nops, int gwarp, int nwarps,
+                                      int cb0, int cbstep, double* red) {
+  for (int i = 0; i < nops; i++) {
+    oz_slice_a<S>(ops[i].A, ops[i].lda, oz[i].s, const_cast<int8_t*>(oz[i].a_planes), const_cast<int*>(oz[i].ea),
+                  gwarp, nwarps);
+    for (int cb = cb0; cb < (ops[i].N + 31) / 32; cb += cbstep)
+      oz_slice_b_block<S>(ops[i].B, ops[i].ldb, oz[i].s, const_cast<int8_t*>(oz[i].b_planes),
+                          const_cast<int*>(oz[i].fb), cb, red);
+  }
+}
+
+__device__ inline void oz_slice_ops(int S, const GemmOp<cplx>* ops, const OzOp* oz, int nops, int gwarp, int nwarps,
+                                    int cb0, int cbstep, double* red) {
+  switch (S) {
+    case 1: oz_slice_ops_s<1>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
+    case 2: oz_slice_ops_s<2>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
+    case 3: oz_slice_ops_s<3>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
+    case 4: oz_slice_ops_s<4>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
+    case 5: oz_slice_ops_s<5>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
+    case 6: oz_slice_ops_s<6>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
+    case 7: oz_slice_ops_s<7>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
+    default: oz_slice_ops_s<8>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
+  }
+}
+
 // Up to 2 independent complex block products C = beta D + alpha A B on the
 // int8 tensor cores, spread over a team of CTAs (the mixed-precision form of
 // team_gemm).  Two phases: digits and exponents of every operand (A rows over
@@ -607,15 +644,8 @@ __device__ bool team_gemm_ozaki(Team& team, const GemmOp<cplx>* ops, int nops, i
     p = oz_bind(oz[i], g.M, g.N, g.K, S, p, g.alpha, g.beta, g.D, g.ldd, g.C, g.ldc);
   }
   const int warps = blockDim.x >> 5;
-  const int gwarp = team.rank() * warps + (threadIdx.x >> 5), nwarps = team.size() * warps;
-  double* red = reinterpret_cast<double*>(smem);
-  for (int i = 0; i < nops; i++) {
-    oz_slice_a(ops[i].A, ops[i].lda, oz[i].s, const_cast<int8_t*>(oz[i].a_planes), const_cast<int*>(oz[i].ea),
-               gwarp, nwarps);
-    for (int cb = team.rank(); cb < (ops[i].N + 31) / 32; cb += team.size())
-      oz_slice_b_block(ops[i].B, ops[i].ldb, oz[i].s, const_cast<int8_t*>(oz[i].b_planes),
-                       const_cast<int*>(oz[i].fb), cb, red);
-  }
+  oz_slice_ops(S, ops, oz, nops, team.rank() * warps + (threadIdx.x >> 5), team.size() * warps, team.rank(),
+               team.size(), reinterpret_cast<double*>(smem));
   // the planes are read by the bulk-copy (async) proxy of every CTA of the team
   asm volatile("fence.proxy.async.global;" ::: "memory");
   if (!team.sync()) return false;
