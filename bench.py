@@ -343,22 +343,12 @@ def run_sinvb(args, rank, world, local_rank):
     # the plain per-matrix FP64 path (one library call per instance, the whole
     # GPU on each matrix) over the same batch, one pass, same in-place inputs
     if not args.no_plain:
-        plain_ms = 0.0
-        for wi, plan in enumerate(plans):
-            generate(wi)
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
-            e0.record(stream)
-            for (d, u, l) in plan.inputs:
-                rgf.rgf_blocks(d, u, l, check=False, overwrite_a=True)
-            e1.record(stream)
-            e1.synchronize()
-            plain_ms += e0.elapsed_time(e1)
+        plain_ms = plain_pass(torch, rgf, plans, generate, stream)
         plain = args.count / (plain_ms * 1e-3)
         out["vs_plain_fp64"] = {"batched": value / world, "plain_per_matrix_fp64": plain,
                                 "ratio": value / world / plain, "sample": "the whole batch, one pass"}
 
-    del pin, plans, plan   # `plan` (loop variable) holds views of the pool too
+    del pin, plans, plan, generate   # `plan` (loop variable) and `generate` hold the pool too
     torch.cuda.empty_cache()
     # accuracy of this precision against the FP64 path, on a sample of the batch
     if args.precision != "fp64":
@@ -369,6 +359,25 @@ def run_sinvb(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(spec)
     return out
+
+
+def plain_pass(torch, rgf, plans, generate, stream):
+    """Device ms of one pass of the plain per-matrix FP64 path (one library call
+    per instance, the whole GPU on each matrix) over the batch, in place on
+    freshly generated inputs.  A function of its own so that no loop variable
+    outlives it holding a view of the input pool."""
+    plain_ms = 0.0
+    for wi, plan in enumerate(plans):
+        generate(wi)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+        e0.record(stream)
+        for (d, u, l) in plan.inputs:
+            rgf.rgf_blocks(d, u, l, check=False, overwrite_a=True)
+        e1.record(stream)
+        e1.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+    return plain_ms
 
 
 def mixed_accuracy(torch, spec, args, dev):

@@ -47,6 +47,10 @@ struct BatchEntry {
 };
 static_assert(sizeof(BatchEntry<cplx>) == 80, "80-byte entries");
 
+// Smallest block size whose products a mixed-precision batch runs on the int8
+// tensor cores (measured on B200: at b = 256 both paths take the same time).
+constexpr int kMixedMinB = 256;
+
 // Digits of the mixed-precision products (flags bits 12-15; 0 means 7).
 __host__ __device__ inline int mixed_digits(unsigned flags) {
   const int d = (int)((flags >> 12) & 15u);
@@ -144,7 +148,9 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
     p.flags = flags;
     p.ckpt = nullptr;
     p.ckpt_every = 1;
-    p.oz_digits = oz_digits;
+    // blocks below kMixedMinB: the int8 path's fixed costs (digit slicing,
+    // pipeline fill) outweigh its faster products, FP64 DMMA is quicker
+    p.oz_digits = e.b >= kMixedMinB ? oz_digits : 0;
     p.oz_scratch = slot + fp64_slot_bytes(e.n, e.b, sizeof(T), save);
     p.oz = &oz_state;
     if (e.b <= 32)
@@ -185,7 +191,7 @@ static BatchLayout batch_layout(const sinvb_batch_desc* d, int count, int dtype,
   size_t slot = 0;
   for (int k = 0; k < count; k++) {
     size_t s = fp64_slot_bytes(d[k].n, d[k].b, es, save);
-    if (mixed) s += 2 * oz_op_scratch(d[k].b, d[k].b, d[k].b, mixed_digits(flags));
+    if (mixed && d[k].b >= kMixedMinB) s += 2 * oz_op_scratch(d[k].b, d[k].b, d[k].b, mixed_digits(flags));
     slot = std::max(slot, s);
   }
   L.nslots = batch_slots();
@@ -231,7 +237,8 @@ static int launch_batched(void* ws, int count, unsigned flags, cudaStream_t stre
   const bool mixed = std::is_same<T, cplx>::value && (flags & SINVB_PREC_MIXED);
   auto k = mixed ? rgf_batched_kernel<T, std::is_same<T, cplx>::value> : rgf_batched_kernel<T, false>;
   size_t smem = kBatchedSmem;
-  if (flags & SINVB_PREC_MIXED) smem = std::max(smem, oz_smem_bytes(mixed_digits(flags)));
+  if (flags & SINVB_PREC_MIXED)
+    smem = std::max(smem, std::max(oz_smem_bytes(mixed_digits(flags)), oz_slice_smem(mixed_digits(flags))));
   SINVB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   // reset status, barrier and queue, and every instance's team area
   SINVB_CUDA(cudaMemsetAsync(ws, 0, 16, stream));

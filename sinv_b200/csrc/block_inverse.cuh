@@ -14,10 +14,11 @@
 //   (ty, tx) of a 16 x 16 grid owns rows ty+16r and columns tx+16c); row k,
 //   column k and 1/a_kk are published through double-buffered shared arrays,
 //   so one barrier per step suffices.
-// * team_invert: any m.  Blocked Gauss-Jordan over 32-wide panels:
-//   (1) invert the diagonal panel block with cta_gj_invert,
+// * team_invert: any m.  Blocked Gauss-Jordan over PW-wide panels:
+//   (1) invert the diagonal panel block (cta_gj_invert for PW <= 64; for
+//       PW = 128 by the whole team, recursively in 64-wide panels),
 //   (2) scale the row panel by it (DMMA GEMM) into a side buffer,
-//   (3) rank-32 update of every other block and the new column panel
+//   (3) rank-PW update of every other block and the new column panel
 //       (DMMA GEMMs), the column panel going to a side buffer; both panels
 //       are copied back while the next pivot block is inverted.
 #pragma once
@@ -29,12 +30,14 @@ namespace sinvb {
 // Blocks of at most kGjMax rows are inverted unblocked by one CTA.  Larger
 // blocks go in panels: the explicit inverse of each pivot block costs accuracy
 // on blocks far from diagonal dominance.  RGF inverts the damped Schur
-// complements S_i and keeps 64-wide panels (tight-binding: ~1e-12 vs 2e-13
-// unblocked); BCR inverts raw reduced diagonal blocks, where 64-wide panels
-// lost three digits (1.8e-9 vs 3e-12) and 32-wide panels lose about one.
+// complements S_i with 128-wide panels whose pivot blocks are themselves
+// inverted in 64-wide panels (the same 64 x 64 pivot inverses as 64-wide
+// panels; tight-binding: ~1e-12 vs 2e-13 unblocked); BCR inverts raw reduced
+// diagonal blocks, where 64-wide panels lost three digits (1.8e-9 vs 3e-12)
+// and 32-wide panels lose about one.
 constexpr int kGjMax = 64;
 constexpr int kPanelRgf = 64;
-constexpr int kPanel = 32;  // BCR
+constexpr int kPanel = 32;      // BCR
 
 template <class T>
 struct GjShared {
@@ -137,10 +140,17 @@ __device__ void team_copy(Team& team, int rows, int cols, const T* src, int lds,
   }
 }
 
-// Elements of side buffer team_invert needs for an m x m block: the new
-// column panel W (m x PW, leading dimension PW) and the scaled row panel R
-// (PW x m, leading dimension m), for the widest panel PW = 64.
-__host__ __device__ inline size_t invert_side_elems(int m) { return m > kGjMax ? 2 * (size_t)m * 64 : 0; }
+// Elements of side buffer team_invert needs for an m x m block with panels of
+// PW: the new column panel W (m x PW, leading dimension PW), the scaled row
+// panel R (PW x m, leading dimension m) and, when PW > kGjMax, the side
+// buffer of the nested inversion of a PW x PW pivot block (panels of PW / 2).
+__host__ __device__ constexpr size_t invert_side_elems_pw(int m, int PW) {
+  return m <= kGjMax ? 0
+                     : (m <= PW && PW > kGjMax) ? invert_side_elems_pw(m, PW / 2)
+                                                : 2 * (size_t)m * PW + (PW > kGjMax ? invert_side_elems_pw(PW, PW / 2) : 0);
+}
+// ... for the widest panels used (RGF)
+__host__ __device__ inline size_t invert_side_elems(int m) { return invert_side_elems_pw(m, kPanelRgf); }
 
 // Inverts the m x m block at a (lda) in place with the whole team.  `side` holds
 // invert_side_elems(m) elements.  Starts and ends with the block visible to the
@@ -159,8 +169,12 @@ __device__ bool team_invert(Team& team, T* a, int lda, int m, T* side, int* stat
     if (team.rank() == 0) cta_gj_invert<T>(a, lda, m, status, smem);
     return team.sync();
   }
+  if constexpr (PW > kGjMax) {
+    if (m <= PW) return team_invert<T, BM, BN, PW / 2>(team, a, lda, m, side, status, smem);
+  }
   T* W = side;                       // m x PW
   T* R = side + (size_t)m * PW;      // PW x m, leading dimension m
+  T* inner = R + (size_t)PW * m;     // nested pivot-block inversion (PW > kGjMax)
   const int np = (m + PW - 1) / PW;
   int pK0 = -1, pkb = 0;
   auto write_back = [&]() {
@@ -173,9 +187,17 @@ __device__ bool team_invert(Team& team, T* a, int lda, int m, T* side, int* stat
   for (int p = 0; p < np; p++) {
     const int K0 = p * PW, kb = min(PW, m - K0), right = K0 + kb;
     T* Dinv = a + (size_t)K0 * lda + K0;
-    if (team.rank() == 0) cta_gj_invert<T>(Dinv, lda, kb, status, smem);
-    if (pK0 >= 0) write_back();
-    if (!team.sync()) return false;
+    if constexpr (PW > kGjMax) {
+      // the whole team inverts the pivot block (64-wide panels) after the
+      // previous panel is written back
+      if (pK0 >= 0) write_back();
+      if (!team.sync()) return false;
+      if (!team_invert<T, BM, BN, PW / 2>(team, Dinv, lda, kb, inner, status, smem)) return false;
+    } else {
+      if (team.rank() == 0) cta_gj_invert<T>(Dinv, lda, kb, status, smem);
+      if (pK0 >= 0) write_back();
+      if (!team.sync()) return false;
+    }
     {
       GemmOp<T> ops[2];
       ops[0] = make_op<T>(kb, K0, kb, 1.0, Dinv, lda, a + (size_t)K0 * lda, lda, nullptr, 0, R, m);

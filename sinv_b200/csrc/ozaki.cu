@@ -11,16 +11,15 @@ namespace sinvb {
 // order oz_bind lays them out.
 static size_t oz_workspace_bytes(int M, int N, int K, int S) { return sizeof(WsHeader) + oz_op_scratch(M, N, K, S); }
 
-// Digits of both operands: CTAs [0, ctas_a) take A rows (one warp per row),
-// the rest one 32-column block of B each.
+// Digits of both operands: CTAs [0, ctas_a) take groups of 8 A rows, the
+// others 32-column blocks of B.
 __global__ void __launch_bounds__(256) oz_slice_kernel(GemmOp<cplx> g, OzOp op, int ctas_a) {
-  __shared__ double red[256];
-  if ((int)blockIdx.x < ctas_a) {
-    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (ctas_a * blockDim.x) >> 5;
-    oz_slice_ops(op.s.S, &g, &op, 1, gwarp, nwarps, 1 << 30, 1, red);  // A only
-  } else {
-    oz_slice_ops(op.s.S, &g, &op, 1, 1 << 30, 1, blockIdx.x - ctas_a, 1 << 30, red);  // one B block
-  }
+  extern __shared__ __align__(16) unsigned char slice_smem[];
+  const int never = 1 << 30;
+  if ((int)blockIdx.x < ctas_a)
+    oz_slice_ops(op.s.S, &g, &op, 1, blockIdx.x, ctas_a, never, 1, slice_smem);
+  else
+    oz_slice_ops(op.s.S, &g, &op, 1, never, 1, blockIdx.x - ctas_a, gridDim.x - ctas_a, slice_smem);
 }
 
 // Persistent over output tiles: every CTA allocates TMEM once and walks tiles
@@ -62,11 +61,15 @@ int sinvb_zgemm_ozaki(int M, int N, int K, double alpha, const void* A, int lda,
   const int sms = device_sm_count();
   OzOp op;
   oz_bind(op, M, N, K, digits, ws + sizeof(WsHeader), alpha, beta, (const cplx*)D, ldd, (cplx*)C, ldc);
-  int ctas_a = (M + 7) / 8;  // one warp per row, 8 warps per CTA
-  if (ctas_a > sms * 4) ctas_a = sms * 4;
+  int ctas_a = (M + 7) / 8;  // one CTA per group of 8 rows
+  if (ctas_a > sms) ctas_a = sms;
+  int ctas_b = (N + 31) / 32;  // one CTA per 32-column block
+  if (ctas_b > sms) ctas_b = sms;
   const GemmOp<cplx> g = make_op<cplx>(M, N, K, alpha, (const cplx*)A, lda, (const cplx*)B, ldb, (const cplx*)D, ldd,
                                        (cplx*)C, ldc);
-  oz_slice_kernel<<<ctas_a + (N + 31) / 32, 256, 0, st>>>(g, op, ctas_a);
+  const size_t slice_smem = oz_slice_smem(digits);
+  SINVB_CUDA(cudaFuncSetAttribute(oz_slice_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slice_smem));
+  oz_slice_kernel<<<ctas_a + ctas_b, 256, slice_smem, st>>>(g, op, ctas_a);
   SINVB_CUDA(cudaGetLastError());
   const size_t smem = oz_smem_bytes(digits);
   SINVB_CUDA(cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

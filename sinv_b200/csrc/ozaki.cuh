@@ -77,7 +77,8 @@ __host__ __device__ inline OzShape oz_shape(int M, int N, int K, int S) {
 // Stages of the ring: four, three for 8 digits (shared memory).
 __host__ __device__ constexpr int oz_stages(int S) { return S <= 7 ? 4 : 3; }
 __host__ __device__ constexpr size_t oz_stage_bytes(int S) { return (size_t)S * (kOzStageA + kOzStageB); }
-// ring, epilogue staging, 128 exponents of the tile being written
+// ring, epilogue staging, 128 exponents of the tile being written (the
+// slicing phase reuses the same space, see oz_slice_smem)
 __host__ __device__ constexpr size_t oz_smem_bytes(int S) {
   return oz_stages(S) * oz_stage_bytes(S) + kOzEpiBytes + 128 * sizeof(int);
 }
@@ -133,140 +134,157 @@ __device__ __forceinline__ uint32_t oz_pack4(int b0, int b1, int b2, int b3) {
   return __byte_perm(__byte_perm(b0, b1, 0x0040), __byte_perm(b2, b3, 0x0040), 0x5410);
 }
 
-// Writes the digits of 4 consecutive K (Re x[q], Im y[q]) of one complex row
-// of A into both embedded rows.
-template <int S>
-__device__ __forceinline__ void oz_store_a4(int8_t* planes, const OzShape& s, int rre, int k4, const double (&x)[4],
-                                            const double (&y)[4]) {
-  int dx[4][S], dy[4][S];
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    oz_split<S>(x[q], dx[q]);
-    oz_split<S>(y[q], dy[q]);
-  }
-  const int rim = rre + kOzTileM;
-  const size_t o_rr = oz_off(rre, k4, s.Mp), o_rn = oz_off(rre, s.Kh + k4, s.Mp);
-  const size_t o_ir = oz_off(rim, k4, s.Mp), o_in = oz_off(rim, s.Kh + k4, s.Mp);
-#pragma unroll
-  for (int t = 0; t < S; t++) {
-    const uint32_t wr = oz_pack4(dx[0][t], dx[1][t], dx[2][t], dx[3][t]);
-    const uint32_t wi = oz_pack4(dy[0][t], dy[1][t], dy[2][t], dy[3][t]);
-    const uint32_t wn = __vsub4(0u, wi);  // bytewise -Im
-    int8_t* pl = planes + (size_t)t * s.a_plane();
-    *reinterpret_cast<uint32_t*>(pl + o_rr) = wr;  // [Re A | -Im A]
-    *reinterpret_cast<uint32_t*>(pl + o_rn) = wn;
-    *reinterpret_cast<uint32_t*>(pl + o_ir) = wi;  // [Im A |  Re A]
-    *reinterpret_cast<uint32_t*>(pl + o_in) = wr;
-  }
-}
+// A side, by CTAs: CTA-group g holds the 8 complex rows 8g .. 8g+7 (warp w
+// loads row 8g + w, lane l the K = 4l + 128m + q, q < 4, so each load of a
+// warp is one contiguous 2 KB run), whose embedded rows form two whole 8-row
+// groups of the planes.  The digits of a chunk of kOzAChunk K are assembled in
+// shared memory as core matrices (8 rows x 16 bytes, padded to 144 bytes so
+// the 4-byte writes of a warp hit 32 banks) and copied out with 16-byte
+// stores, eight lanes per 128-byte core matrix.  Rows past M are written as
+// zeros (they only reach output rows that are never stored).
+constexpr int kOzAChunk = 512;                  // K per staging pass (4 x 128)
+constexpr int kOzCmStride = 144;                // staged bytes per core matrix
+constexpr int kOzACms = kOzAChunk / 16;         // core matrices per (digit, row group, half)
+__host__ __device__ constexpr size_t oz_slice_a_smem(int S) { return (size_t)S * 4 * kOzACms * kOzCmStride; }
 
-// A side: exponents e_i and the digit planes of the embedded rows.  One warp
-// per complex row (warp `gwarp` of `nwarps`); lane l takes K = 4l + 128m + q
-// (q < 4), so every load of the warp is one contiguous 2 KB run.  Rows of up to
-// kOzRowRegs x 128 entries are read once and held in registers; longer rows
-// are read a second time for the digits.  Rows past M are left unwritten: they
-// only reach output rows that are never stored.
-constexpr int kOzRowRegs = 4;
 template <int S>
-__device__ inline void oz_slice_a(const cplx* A, int lda, const OzShape& s, int8_t* planes, int* ea, int gwarp,
-                                  int nwarps) {
-  const int lane = threadIdx.x & 31;
-  const int chunks = (s.Kh + 127) / 128;
-  for (int i = gwarp; i < s.M; i += nwarps) {
+__device__ inline void oz_slice_a(const cplx* A, int lda, const OzShape& s, int8_t* planes, int* ea, int g0,
+                                  int gstep, unsigned char* stage) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int groups = (s.M + 7) / 8;
+  for (int g = g0; g < groups; g += gstep) {
+    const int i = 8 * g + warp;
+    const bool live = i < s.M;
     const cplx* row = A + (size_t)i * lda;
-    cplx v[kOzRowRegs][4];
+    cplx v[4][4];
     double amax = 0.0;
 #pragma unroll
-    for (int m = 0; m < kOzRowRegs; m++)
+    for (int m = 0; m < 4; m++)
 #pragma unroll
       for (int q = 0; q < 4; q++) {
         const int k = 128 * m + 4 * lane + q;
-        v[m][q] = (m < chunks && k < s.K) ? row[k] : cplx{0.0, 0.0};
+        v[m][q] = (live && k < s.K) ? row[k] : cplx{0.0, 0.0};
         amax = fmax(amax, fmax(fabs(v[m][q].re), fabs(v[m][q].im)));
       }
-    for (int m = kOzRowRegs; m < chunks; m++)
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int k = 128 * m + 4 * lane + q;
-        if (k < s.K) {
-          const cplx w = row[k];
-          amax = fmax(amax, fmax(fabs(w.re), fabs(w.im)));
-        }
-      }
+    for (int k = kOzAChunk + lane; live && k < s.K; k += 32) {
+      const cplx w = row[k];
+      amax = fmax(amax, fmax(fabs(w.re), fabs(w.im)));
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
     const int e = oz_exponent(amax);
-    if (lane == 0) ea[i] = e;
+    if (lane == 0 && live) ea[i] = e;
     const double sc = ldexp(1.0, -e);
-    const int rre = (i / kOzTileM) * 2 * kOzTileM + i % kOzTileM;
+    const int gre = (8 * g / kOzTileM) * 2 * kOzTileM + (8 * g) % kOzTileM;  // first embedded row (Re part)
+    for (int k0 = 0; k0 < s.Kh; k0 += kOzAChunk) {
+      if (k0 > 0) {
 #pragma unroll
-    for (int m = 0; m < kOzRowRegs; m++) {
-      const int k4 = 128 * m + 4 * lane;
-      if (m < chunks && k4 < s.Kh) {
-        double x[4], y[4];
+        for (int m = 0; m < 4; m++)
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-          x[q] = v[m][q].re * sc;
-          y[q] = v[m][q].im * sc;
-        }
-        oz_store_a4<S>(planes, s, rre, k4, x, y);
+          for (int q = 0; q < 4; q++) {
+            const int k = k0 + 128 * m + 4 * lane + q;
+            v[m][q] = (live && k < s.K) ? row[k] : cplx{0.0, 0.0};
+          }
       }
-    }
-    for (int m = kOzRowRegs; m < chunks; m++) {
-      const int k4 = 128 * m + 4 * lane;
-      if (k4 < s.Kh) {
-        double x[4], y[4];
+      const int kc = s.Kh - k0 < kOzAChunk ? s.Kh - k0 : kOzAChunk;  // multiple of 16
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const int k = k4 + q;
-          const cplx w = k < s.K ? row[k] : cplx{0.0, 0.0};
-          x[q] = w.re * sc;
-          y[q] = w.im * sc;
+      for (int m = 0; m < 4; m++) {
+        const int kk = 128 * m + 4 * lane;  // within the chunk
+        if (kk < kc) {
+          int dx[4][S], dy[4][S];
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            oz_split<S>(v[m][q].re * sc, dx[q]);
+            oz_split<S>(v[m][q].im * sc, dy[q]);
+          }
+          // staging index: [digit][group: 0 = Re rows, 1 = Im rows][half][core matrix]
+          const int cm = kk >> 4, byte = warp * 16 + (kk & 15);
+#pragma unroll
+          for (int t = 0; t < S; t++) {
+            const uint32_t wr = oz_pack4(dx[0][t], dx[1][t], dx[2][t], dx[3][t]);
+            const uint32_t wi = oz_pack4(dy[0][t], dy[1][t], dy[2][t], dy[3][t]);
+            unsigned char* b0 = stage + (size_t)t * 4 * kOzACms * kOzCmStride + cm * kOzCmStride + byte;
+            *reinterpret_cast<uint32_t*>(b0) = wr;                                        // Re rows, first half
+            *reinterpret_cast<uint32_t*>(b0 + 1 * kOzACms * kOzCmStride) = __vsub4(0u, wi);  // Re rows, -Im
+            *reinterpret_cast<uint32_t*>(b0 + 2 * kOzACms * kOzCmStride) = wi;            // Im rows, Im
+            *reinterpret_cast<uint32_t*>(b0 + 3 * kOzACms * kOzCmStride) = wr;            // Im rows, Re
+          }
         }
-        oz_store_a4<S>(planes, s, rre, k4, x, y);
       }
+      __syncthreads();
+      // copy out: item = (digit, quarter, core matrix, row); 16 bytes each
+      const int ncm = kc / 16, items = S * 4 * ncm * 8;
+      for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int r8 = it & 7, rest = it >> 3;
+        const int cm = rest % ncm, qt = (rest / ncm) & 3, t = rest / ncm / 4;
+        const int rowe = gre + (qt >> 1) * kOzTileM + r8;       // embedded row
+        const int kp = (qt & 1) * s.Kh + k0 + 16 * cm;          // K' byte
+        const uint4 w = *reinterpret_cast<const uint4*>(stage + ((size_t)(t * 4 + qt) * kOzACms + cm) * kOzCmStride +
+                                                        r8 * 16);
+        *reinterpret_cast<uint4*>(planes + (size_t)t * s.a_plane() + oz_off(rowe, kp, s.Mp)) = w;
+      }
+      __syncthreads();
     }
   }
 }
 
-// B side for the 32 columns [32 cb, 32 cb + 32): column exponents f_j (warps
-// split the rows, lanes are columns, then a reduction in shared memory), then
-// the digit planes of the B^T rows [Re B(:,j) | Im B(:,j)] (each thread 16
-// consecutive K of one column, one 16-byte store per digit and half).  Called
-// by every thread of the CTA; `red` is blockDim.x doubles of shared memory.
-// Columns past N are left unwritten (they only reach discarded outputs).
+// B side for the 32-column blocks cb0, cb0 + cbstep, ... (up to 4 at a time):
+// column exponents f_j (warps split the rows, each lane keeps the maxima of
+// one column per block, then a reduction in shared memory), then the digit
+// planes of the B^T rows [Re B(:,j) | Im B(:,j)] (each thread 16 consecutive K
+// of one column, one 16-byte store per digit and half; eight lanes fill one
+// 128-byte core matrix).  Called by every thread of the CTA; `red` is
+// 4 x blockDim.x doubles of shared memory.  Columns past N are left unwritten
+// (they only reach discarded outputs).
 template <int S>
-__device__ inline void oz_slice_b_block(const cplx* B, int ldb, const OzShape& s, int8_t* planes, int* fb, int cb,
-                                        double* red) {
+__device__ inline void oz_slice_b(const cplx* B, int ldb, const OzShape& s, int8_t* planes, int* fb, int cb0, int cbstep,
+                                  double* red) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const int j = cb * 32 + lane;
-  const bool valid = j < s.N;
-  double amax = 0.0;
-  if (valid) {
-#pragma unroll 8
-    for (int k = warp; k < s.K; k += nw) {
-      const cplx v = B[(size_t)k * ldb + j];
-      amax = fmax(amax, fmax(fabs(v.re), fabs(v.im)));
-    }
-  }
-  red[warp * 32 + lane] = amax;
-  __syncthreads();
-  if (warp == 0) {
-    for (int w = 1; w < nw; w++) amax = fmax(amax, red[w * 32 + lane]);
-    const int f = oz_exponent(amax);
-    if (valid) fb[j] = f;
-    red[lane] = ldexp(1.0, -f);
-  }
-  __syncthreads();
-  const double sc = red[lane];
-  for (int k16 = 16 * warp; k16 < s.Kh; k16 += 16 * nw) {
-    cplx v[16];
+  const int blocks = (s.N + 31) / 32;
+  for (int cb1 = cb0; cb1 < blocks; cb1 += 4 * cbstep) {
+    int js[4];
+    double amax[4];
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
-      const int k = k16 + q;
-      v[q] = (valid && k < s.K) ? B[(size_t)k * ldb + j] : cplx{0.0, 0.0};
+    for (int r = 0; r < 4; r++) {
+      const int cb = cb1 + r * cbstep;
+      js[r] = cb < blocks ? cb * 32 + lane : s.N;
+      amax[r] = 0.0;
     }
-    if (valid) {
+#pragma unroll 4
+    for (int k = warp; k < s.K; k += nw) {
+#pragma unroll
+      for (int r = 0; r < 4; r++)
+        if (js[r] < s.N) {
+          const cplx v = B[(size_t)k * ldb + js[r]];
+          amax[r] = fmax(amax[r], fmax(fabs(v.re), fabs(v.im)));
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++) red[(r * nw + warp) * 32 + lane] = amax[r];
+    __syncthreads();
+    if (warp < 4) {  // warp r finishes block r
+      const int r = warp;
+      double mx = 0.0;
+      for (int w = 0; w < nw; w++) mx = fmax(mx, red[(r * nw + w) * 32 + lane]);
+      const int f = oz_exponent(mx);
+      const int cb = cb1 + r * cbstep, j = cb * 32 + lane;
+      if (cb < blocks && j < s.N) fb[j] = f;
+      red[4 * nw * 32 + r * 32 + lane] = ldexp(1.0, -f);
+    }
+    __syncthreads();
+    const int per = s.Kh / 16;  // 16-K groups per column
+    for (int w = warp; w < 4 * per; w += nw) {
+      const int r = w / per, k16 = 16 * (w % per);
+      const int j = js[r];
+      if (j >= s.N) continue;  // warp-uniform: whole block past N
+      const double sc = red[4 * nw * 32 + r * 32 + lane];
+      const bool valid = j < s.N;
+      cplx v[16];
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        const int k = k16 + q;
+        v[q] = (valid && k < s.K) ? B[(size_t)k * ldb + j] : cplx{0.0, 0.0};
+      }
       uint32_t wr[S][4], wi[S][4];
 #pragma unroll
       for (int g = 0; g < 4; g++) {
@@ -282,16 +300,18 @@ __device__ inline void oz_slice_b_block(const cplx* B, int ldb, const OzShape& s
           wi[t][g] = oz_pack4(dy[0][t], dy[1][t], dy[2][t], dy[3][t]);
         }
       }
-      const size_t o_r = oz_off(j, k16, s.Np), o_i = oz_off(j, s.Kh + k16, s.Np);
+      if (valid) {
+        const size_t o_r = oz_off(j, k16, s.Np), o_i = oz_off(j, s.Kh + k16, s.Np);
 #pragma unroll
-      for (int t = 0; t < S; t++) {
-        int8_t* pl = planes + (size_t)t * s.b_plane();
-        *reinterpret_cast<uint4*>(pl + o_r) = make_uint4(wr[t][0], wr[t][1], wr[t][2], wr[t][3]);
-        *reinterpret_cast<uint4*>(pl + o_i) = make_uint4(wi[t][0], wi[t][1], wi[t][2], wi[t][3]);
+        for (int t = 0; t < S; t++) {
+          int8_t* pl = planes + (size_t)t * s.b_plane();
+          *reinterpret_cast<uint4*>(pl + o_r) = make_uint4(wr[t][0], wr[t][1], wr[t][2], wr[t][3]);
+          *reinterpret_cast<uint4*>(pl + o_i) = make_uint4(wi[t][0], wi[t][1], wi[t][2], wi[t][3]);
+        }
       }
     }
+    __syncthreads();  // `red` is reused by the next batch of blocks
   }
-  __syncthreads();  // `red` is reused by the next column block
 }
 
 // Per-CTA state of the tile pipeline; lives in shared memory for the whole kernel.
@@ -598,39 +618,42 @@ __host__ __device__ inline unsigned char* oz_bind(OzOp& o, int M, int N, int K, 
   return p;
 }
 
-// Digits and exponents of the operands of `nops` products: A rows over warp
-// `gwarp` of `nwarps`, B column blocks cb0, cb0 + cbstep, ... (every thread of
-// a CTA calls this with the same cb0 / cbstep).
+// Digits and exponents of the operands of `nops` products: A row groups
+// a0, a0 + astep, ..., B column blocks b0, b0 + bstep, ...  Called by every
+// thread of the CTA; `smem` holds oz_slice_smem(S) bytes.
+__host__ __device__ constexpr size_t oz_slice_smem(int S) {
+  return oz_slice_a_smem(S) > 4 * 256 * 8 + 4 * 32 * 8 ? oz_slice_a_smem(S) : 4 * 256 * 8 + 4 * 32 * 8;
+}
+
 template <int S>
-__device__ inline void oz_slice_ops_s(const GemmOp<cplx>* ops, const OzOp* oz, int nops, int gwarp, int nwarps,
-                                      int cb0, int cbstep, double* red) {
+__device__ inline void oz_slice_ops_s(const GemmOp<cplx>* ops, const OzOp* oz, int nops, int a0, int astep, int b0,
+                                      int bstep, unsigned char* smem) {
   for (int i = 0; i < nops; i++) {
-    oz_slice_a<S>(ops[i].A, ops[i].lda, oz[i].s, const_cast<int8_t*>(oz[i].a_planes), const_cast<int*>(oz[i].ea),
-                  gwarp, nwarps);
-    for (int cb = cb0; cb < (ops[i].N + 31) / 32; cb += cbstep)
-      oz_slice_b_block<S>(ops[i].B, ops[i].ldb, oz[i].s, const_cast<int8_t*>(oz[i].b_planes),
-                          const_cast<int*>(oz[i].fb), cb, red);
+    oz_slice_a<S>(ops[i].A, ops[i].lda, oz[i].s, const_cast<int8_t*>(oz[i].a_planes), const_cast<int*>(oz[i].ea), a0,
+                  astep, smem);
+    oz_slice_b<S>(ops[i].B, ops[i].ldb, oz[i].s, const_cast<int8_t*>(oz[i].b_planes), const_cast<int*>(oz[i].fb), b0,
+                  bstep, reinterpret_cast<double*>(smem));
   }
 }
 
-__device__ inline void oz_slice_ops(int S, const GemmOp<cplx>* ops, const OzOp* oz, int nops, int gwarp, int nwarps,
-                                    int cb0, int cbstep, double* red) {
+__device__ inline void oz_slice_ops(int S, const GemmOp<cplx>* ops, const OzOp* oz, int nops, int a0, int astep,
+                                    int b0, int bstep, unsigned char* smem) {
   switch (S) {
-    case 1: oz_slice_ops_s<1>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
-    case 2: oz_slice_ops_s<2>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
-    case 3: oz_slice_ops_s<3>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
-    case 4: oz_slice_ops_s<4>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
-    case 5: oz_slice_ops_s<5>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
-    case 6: oz_slice_ops_s<6>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
-    case 7: oz_slice_ops_s<7>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
-    default: oz_slice_ops_s<8>(ops, oz, nops, gwarp, nwarps, cb0, cbstep, red); break;
+    case 1: oz_slice_ops_s<1>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
+    case 2: oz_slice_ops_s<2>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
+    case 3: oz_slice_ops_s<3>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
+    case 4: oz_slice_ops_s<4>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
+    case 5: oz_slice_ops_s<5>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
+    case 6: oz_slice_ops_s<6>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
+    case 7: oz_slice_ops_s<7>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
+    default: oz_slice_ops_s<8>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
   }
 }
 
 // Up to 2 independent complex block products C = beta D + alpha A B on the
 // int8 tensor cores, spread over a team of CTAs (the mixed-precision form of
-// team_gemm).  Two phases: digits and exponents of every operand (A rows over
-// all warps of the team, B column blocks over its CTAs), then the output tiles
+// team_gemm).  Two phases: digits and exponents of every operand (A row groups
+// and B column blocks over the CTAs of the team), then the output tiles
 // (over its CTAs).  The caller synchronises after the second.  Plain
 // (non-transposed) operands only.  Returns false when a wait gave up.
 template <class Team>
@@ -643,9 +666,7 @@ __device__ bool team_gemm_ozaki(Team& team, const GemmOp<cplx>* ops, int nops, i
     const GemmOp<cplx>& g = ops[i];
     p = oz_bind(oz[i], g.M, g.N, g.K, S, p, g.alpha, g.beta, g.D, g.ldd, g.C, g.ldc);
   }
-  const int warps = blockDim.x >> 5;
-  oz_slice_ops(S, ops, oz, nops, team.rank() * warps + (threadIdx.x >> 5), team.size() * warps, team.rank(),
-               team.size(), reinterpret_cast<double*>(smem));
+  oz_slice_ops(S, ops, oz, nops, team.rank(), team.size(), team.rank(), team.size(), smem);
   // the planes are read by the bulk-copy (async) proxy of every CTA of the team
   asm volatile("fence.proxy.async.global;" ::: "memory");
   if (!team.sync()) return false;

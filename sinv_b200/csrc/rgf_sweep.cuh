@@ -58,24 +58,24 @@ struct RgfParams {
   T* ckpt;         // optional: g_{s*c-1} saved to ckpt[s-1] (s = 1, 2, ...) for the adjoint
   int ckpt_every;  // c
   // mixed precision (complex only): block products on the int8 tensor cores
-  int oz_digits;              // digits of the tensor-core products (used by Mixed sweeps only)
+  int oz_digits;              // digits of the tensor-core products (Mixed sweeps; 0: FP64 products)
   unsigned char* oz_scratch;  // 2 x oz_op_scratch(b, b, b, digits) bytes
   OzState* oz;                // per-CTA pipeline state (TMEM allocated by the kernel)
 };
 
 // The block products of a sweep phase: FP64 DMMA, or (Mixed, complex only)
-// the int8 tensor-core Ozaki products with p.oz_digits (>= 1) digits.  The
-// block inverses always stay in FP64.  Mixed is a template switch so that
-// kernels without the tensor-core path do not carry its registers.
+// the int8 tensor-core Ozaki products when p.oz_digits > 0.  The block
+// inverses always stay in FP64.  Mixed is a template switch so that kernels
+// without the tensor-core path do not carry its registers.
 template <class T, int BM, int BN, bool Mixed, class Team>
 __device__ __forceinline__ bool sweep_gemm(Team& team, const RgfParams<T>& p, const GemmOp<T>* ops, int nops, T* smem) {
   if constexpr (Mixed && std::is_same<T, cplx>::value) {
-    return team_gemm_ozaki(team, ops, nops, p.oz_digits, p.oz_scratch, p.oz, reinterpret_cast<unsigned char*>(smem),
-                           p.status);
-  } else {
-    team_gemm<T, BM, BN>(team, ops, nops, smem);
-    return true;
+    if (p.oz_digits > 0)
+      return team_gemm_ozaki(team, ops, nops, p.oz_digits, p.oz_scratch, p.oz, reinterpret_cast<unsigned char*>(smem),
+                             p.status);
   }
+  team_gemm<T, BM, BN>(team, ops, nops, smem);
+  return true;
 }
 
 template <class T, int BM, int BN, bool Mixed = false, class Team>

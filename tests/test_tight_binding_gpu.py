@@ -16,7 +16,7 @@ from sinv_b200.algorithms import bcr_s, rgf, rgf_batched
 
 pytestmark = pytest.mark.gpu
 
-CASES = [(1, 128), (2, 130), (6, 130), (12, 128), (3, 256), (4, 100)]
+CASES = [(1, 128), (2, 130), (6, 130), (12, 128), (3, 256), (4, 100), (2, 300), (2, 512)]
 
 
 def _worst(G, R):
