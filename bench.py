@@ -11,7 +11,15 @@ the launching stream).  A step is one pass over all 512 instances.  Inputs are
 larger than L2 (126 MB) in every wave.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sinvb|reference]
-                    [--precision fp64|mixed] [--count 512]
+                    [--precision mixed|fp64] [--count 512]
+                    [--workload energy_batch|plain_large|gradient_set|large_mixed]
+
+The default workload is the energy batch in mixed precision (block products
+on the int8 tensor cores for b >= 256, FP64 inverses).  The other workloads:
+plain_large (one n=64, b=256 matrix through the single-matrix FP64 path, and
+bcr), gradient_set (loss and dL/dH over 128 energies through the adjoint,
+forward and backward timed apart) and large_mixed (n=256, b=1024 instances in
+one in-place wave, mixed vs FP64 and the error on a 4-block sub-instance).
 
 Metric: matrices/s of the whole batch (all ranks).  Under torchrun every rank
 processes its own 512-instance batch (different Hamiltonian seeds): weak
@@ -42,9 +50,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="sinvb", choices=["sinvb", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default="energy_batch",
+                    choices=["energy_batch", "plain_large", "gradient_set", "large_mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--digits", type=int, default=7, help="int8 slices per value of the mixed products")
-    ap.add_argument("--count", type=int, default=512)
+    ap.add_argument("--count", type=int, default=0, help="instances (0: the workload's default)")
     ap.add_argument("--shape", default=None, help="n,b: uniform batch of that shape instead of the energy batch")
     ap.add_argument("--wave-gb", type=float, default=0.0, help="input GB per wave (0: as much as HBM holds)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -274,14 +284,12 @@ def run_sinvb(args, rank, world, local_rank):
     waves = make_waves(spec, budget)
     pool_elems = max(sum(in_elems(spec[k][1], spec[k][2]) for k in w) for w in waves)
     pin = torch.empty(pool_elems, dtype=torch.complex128, device=dev)
-    plans = []
-    for w in waves:
-        plans.append(BatchPlan(carve(pin, spec, w), precision=args.precision, inplace=True,
-                               digits=args.digits))
+    views = [carve(pin, spec, w) for w in waves]
+    plans = [BatchPlan(v, precision=args.precision, inplace=True, digits=args.digits) for v in views]
     flops = [sum(workloads.rgf_flops(spec[k][1], spec[k][2]) for k in w) for w in waves]
 
     def generate(wi):
-        for k, (d, u, l) in zip(waves[wi], plans[wi].inputs):
+        for k, (d, u, l) in zip(waves[wi], views[wi]):
             e, n, b, s = spec[k]
             workloads.tight_binding_device(n, b, e, s, device=dev, out=(d, u, l))
 
@@ -343,12 +351,30 @@ def run_sinvb(args, rank, world, local_rank):
     # the plain per-matrix FP64 path (one library call per instance, the whole
     # GPU on each matrix) over the same batch, one pass, same in-place inputs
     if not args.no_plain:
-        plain_ms = plain_pass(torch, rgf, plans, generate, stream)
+        plain_ms = plain_pass(torch, rgf, views, generate, stream)
         plain = args.count / (plain_ms * 1e-3)
         out["vs_plain_fp64"] = {"batched": value / world, "plain_per_matrix_fp64": plain,
                                 "ratio": value / world / plain, "sample": "the whole batch, one pass"}
+    # the batched FP64 path over the same batch, one pass (for the mixed line)
+    if args.precision != "fp64":
+        del plans
+        plans = [BatchPlan(v, precision="fp64", inplace=True) for v in views]
+        f_ms = 0.0
+        for wi, plan in enumerate(plans):
+            generate(wi)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+            e0.record(stream)
+            plan.run(stream)
+            e1.record(stream)
+            e1.synchronize()
+            f_ms += e0.elapsed_time(e1)
+            plan.check()
+        out["batched_fp64"] = {"value": args.count / (f_ms * 1e-3), "unit": UNIT,
+                               "mixed_over_fp64": value / world / (args.count / (f_ms * 1e-3)),
+                               "sample": "the whole batch, one pass"}
 
-    del pin, plans, plan, generate   # `plan` (loop variable) and `generate` hold the pool too
+    del pin, views, plans, plan, generate   # loop variables and `generate` hold the pool too
     torch.cuda.empty_cache()
     # accuracy of this precision against the FP64 path, on a sample of the batch
     if args.precision != "fp64":
@@ -361,18 +387,18 @@ def run_sinvb(args, rank, world, local_rank):
     return out
 
 
-def plain_pass(torch, rgf, plans, generate, stream):
+def plain_pass(torch, rgf, views, generate, stream):
     """Device ms of one pass of the plain per-matrix FP64 path (one library call
     per instance, the whole GPU on each matrix) over the batch, in place on
     freshly generated inputs.  A function of its own so that no loop variable
     outlives it holding a view of the input pool."""
     plain_ms = 0.0
-    for wi, plan in enumerate(plans):
+    for wi, wave in enumerate(views):
         generate(wi)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
         e0.record(stream)
-        for (d, u, l) in plan.inputs:
+        for (d, u, l) in wave:
             rgf.rgf_blocks(d, u, l, check=False, overwrite_a=True)
         e1.record(stream)
         e1.synchronize()
@@ -462,13 +488,330 @@ def e2e_sample(torch, spec, args, dev, world):
     return e2e
 
 
+# --------------------------------------------------------------------------- other workloads
+def _events_ms(torch, fn, stream):
+    e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def _max_over_ranks(torch, world, dev, ms):
+    if world == 1:
+        return ms
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_plain_large(args, rank, world, local_rank):
+    """One matrix n=64, b=256 (diagonally dominant generator, seed 0) through the
+    plain single-matrix FP64 path: rgf, and bcr on the same block arrays.  A step
+    is one selected inversion; every rank inverts its own copy (replicas)."""
+    import torch
+    from sinv_b200 import workloads
+    from sinv_b200.algorithms import bcr_s, rgf
+    from oracle import rgf_oracle
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    n, b = 64, 256
+    dn, un, ln = workloads.dominant(n, b, seed=0)
+    d, u, l = (torch.from_numpy(x).to(dev) for x in (dn, un, ln))
+    peak = dmma_peak_tflops(torch)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MB > L2
+    clocks = Clocks(local_rank) if rank == 0 else None
+    ts, tb = [], []
+    for step in range(args.warmup + args.steps):
+        if step == args.warmup and clocks:
+            clocks.start()
+        flush.zero_()
+        ms = _events_ms(torch, lambda: rgf.rgf_blocks(d, u, l, check=False), stream)
+        flush.zero_()
+        mb = _events_ms(torch, lambda: bcr_s.bcr_blocks(d, u, l, check=False), stream)
+        if step >= args.warmup:
+            ts.append(_max_over_ranks(torch, world, dev, ms))
+            tb.append(_max_over_ranks(torch, world, dev, mb))
+    clk = clocks.stop() if clocks else None
+    G = rgf.rgf_blocks(d, u, l)
+    R = rgf_oracle.rgf(dn, un, ln)
+    err = max(float(np.linalg.norm(g.cpu().numpy() - r) / np.linalg.norm(r)) for g, r in zip(G, R))
+    ms = statistics.median(ts)
+    F = workloads.rgf_flops(n, b)
+    # e2e: host (pinned) inputs in, host outputs back, through the public call
+    hd, hu, hl = (torch.from_numpy(x).pin_memory() for x in (dn, un, ln))
+    te = []
+    for step in range(args.warmup + args.steps):
+        def e2e():
+            G = rgf.rgf_blocks(hd.to(dev, non_blocking=True), hu.to(dev, non_blocking=True),
+                               hl.to(dev, non_blocking=True), check=False)
+            return [g.to("cpu") for g in G]
+        m = _events_ms(torch, e2e, stream)
+        if step >= args.warmup:
+            te.append(m)
+    bytes_in = sum(x.nbytes for x in (dn, un, ln))
+    out = {"metric": "RGF matrices/s, one matrix, plain FP64 path", "value": world / (ms * 1e-3),
+           "unit": "matrices/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+           "data": "synthetic", "config": {"workload": "plain_large(n=64,b=256)", "n": n, "b": b,
+                                           "generator": "diagonally dominant, seed 0",
+                                           "l2": "256 MB buffer written between timed calls",
+                                           "parallelism": "replicas%d" % world},
+           "gpu_launches": args.steps, "rel_err_vs_oracle": err,
+           "roofline": {"bound": "tensor", "achieved": F / (ms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                        "frac": F / (ms * 1e-3) / 1e12 / peak, "traffic": None, "kernel": "rgf_grid_kernel",
+                        "flops": "canonical 8 b^3 (8(n-1)+n)", "peak_source": "sinvb_fp64_mma_peak (DMMA)"},
+           "bcr": {"ms": statistics.median(tb), "matrices_per_s": world / (statistics.median(tb) * 1e-3)},
+           "clocks": clk,
+           "e2e": {"value": world / (statistics.median(te) * 1e-3), "unit": "matrices/s",
+                   "h2d_bytes_per_step": bytes_in, "d2h_bytes_per_step": bytes_in}}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = plain_cpu(dn, un, ln)
+    return out
+
+
+def plain_cpu(dn, un, ln):
+    from oracle import rgf_oracle
+    t0 = time.perf_counter()
+    rgf_oracle.rgf(dn, un, ln)
+    t = time.perf_counter() - t0
+    return {"value": 1.0 / t, "unit": "matrices/s", "cores": _blas_threads(), "kind": "port",
+            "sample": "the whole matrix once (reference rgf restated in numpy/OpenBLAS)"}
+
+
+def _blas_threads():
+    try:
+        from threadpoolctl import threadpool_info
+        return max([i.get("num_threads", 1) for i in threadpool_info() if i.get("user_api") == "blas"] or [1])
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_gradient_set(args, rank, world, local_rank):
+    """Loss L = sum_k -Im Tr sum_i G_ii(E_k) / pi over 128 energies of one shared
+    tight-binding H (n=32, b=128) and dL/dH by the hand-written adjoint.  A step
+    evaluates the loss and the gradient over all energies; energies are split
+    over ranks and one all-reduce sums the gradient (strong scaling).  Forward
+    and backward device times are reported separately."""
+    import torch
+    from sinv_b200 import distributed, workloads
+    from sinv_b200.algorithms import rgf_autograd
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    energies, n, b, hseed = workloads.gradient_set_spec(count=args.count)
+    onsite, coupling = workloads.hamiltonian(n, b, hseed)
+    Hd = torch.from_numpy(onsite).to(dev)
+    Hu = torch.from_numpy(coupling).to(dev)
+    mine = distributed.shard_by_cost([1.0] * len(energies), world, rank)
+    eye = torch.eye(b, dtype=torch.complex128, device=dev)
+    stream = torch.cuda.current_stream()
+    peak = dmma_peak_tflops(torch)
+
+    def step():
+        fwd = bwd = 0.0
+        g_on = torch.zeros_like(Hd)
+        g_cp = torch.zeros_like(Hu)
+        loss = torch.zeros((), dtype=torch.float64, device=dev)
+        for k in mine:
+            E = energies[k]
+            hd = Hd.clone().requires_grad_(True)
+            hu = Hu.clone().requires_grad_(True)
+            e0, e1, e2 = (torch.cuda.Event(True) for _ in range(3))
+            e0.record(stream)
+            dd = (E + 1j * workloads.ETA) * eye - hd.to(torch.complex128)
+            edge = torch.zeros_like(dd)
+            edge[0] = 1j * workloads.SIGMA_EDGE * eye
+            edge[-1] = edge[-1] + 1j * workloads.SIGMA_EDGE * eye
+            Gd, _, _ = rgf_autograd(dd + edge, (-hu.to(torch.complex128)).contiguous(),
+                                    (-hu.transpose(1, 2).to(torch.complex128)).contiguous())
+            lk = -Gd.diagonal(0, 1, 2).imag.sum() / np.pi
+            e1.record(stream)
+            lk.backward()
+            e2.record(stream)
+            e2.synchronize()
+            fwd += e0.elapsed_time(e1)
+            bwd += e1.elapsed_time(e2)
+            loss += lk.detach()
+            g_on += hd.grad
+            g_cp += hu.grad
+        if world > 1:
+            import torch.distributed as dist
+            flat = torch.cat([loss.reshape(1), g_on.reshape(-1), g_cp.reshape(-1)])
+            dist.all_reduce(flat)
+        return fwd, bwd
+
+    clocks = Clocks(local_rank) if rank == 0 else None
+    fw, bw, tot = [], [], []
+    for s_ in range(args.warmup + args.steps):
+        if s_ == args.warmup and clocks:
+            clocks.start()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+        e0.record(stream)
+        f, bk = step()
+        e1.record(stream)
+        e1.synchronize()
+        if s_ >= args.warmup:
+            fw.append(f)
+            bw.append(bk)
+            tot.append(_max_over_ranks(torch, world, dev, e0.elapsed_time(e1)))
+    clk = clocks.stop() if clocks else None
+    ms = statistics.median(tot)
+    f_ms, b_ms = statistics.median(fw), statistics.median(bw)
+    F = workloads.rgf_flops(n, b) * len(mine)
+    return {"metric": "energy-gradient evaluations/s (loss and dL/dH per energy)", "value": len(energies) / (ms * 1e-3),
+            "unit": "energies/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": "gradient_set(128 energies, n=32, b=128)", "energies": len(energies), "n": n,
+                       "b": b, "parallelism": "energies sharded over %d rank(s), one all-reduce" % world},
+            "gpu_launches": 2 * len(mine) * args.steps,
+            "forward_ms": f_ms, "backward_ms": b_ms, "backward_over_forward": b_ms / f_ms,
+            "roofline": {"bound": "tensor", "achieved": F / (f_ms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                         "frac": F / (f_ms * 1e-3) / 1e12 / peak, "traffic": None,
+                         "kernel": "rgf forward sweep with checkpoints (forward only)",
+                         "flops": "canonical 8 b^3 (8(n-1)+n) per energy"},
+            "clocks": clk}
+
+
+def run_large_mixed(args, rank, world, local_rank):
+    """Instances n=256, b=1024 (12.85 GB of input each), tight-binding generator;
+    one wave of `count` instances in place in HBM, mixed precision.  Error of
+    the mixed path on a 4-block sub-instance (n=4, b=1024) against the FP64
+    path and the dense FP64 inverse."""
+    import torch
+    from sinv_b200 import workloads
+    from sinv_b200.algorithms import BatchPlan
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    spec = workloads.large_mixed_spec(count=args.count)
+    if rank:
+        spec = [(e, n, b, s + 100000 * rank) for (e, n, b, s) in spec]
+    peak = dmma_peak_tflops(torch)
+    pool = torch.empty(sum(in_elems(n, b) for (_, n, b, _) in spec), dtype=torch.complex128, device=dev)
+    views = carve(pool, spec, list(range(len(spec))))
+    plans = {"mixed": BatchPlan(views, precision="mixed", inplace=True, digits=args.digits)}
+
+    def generate():
+        for (e, n, b, s), (d, u, l) in zip(spec, views):
+            workloads.tight_binding_device(n, b, e, s, device=dev, out=(d, u, l))
+
+    stream = torch.cuda.current_stream()
+    clocks = Clocks(local_rank) if rank == 0 else None
+    tm = []
+    for step in range(args.warmup + args.steps):
+        generate()
+        torch.cuda.synchronize()
+        if step == args.warmup and clocks:
+            clocks.start()
+        ms = _events_ms(torch, lambda: plans["mixed"].run(stream), stream)
+        if step >= args.warmup:
+            tm.append(_max_over_ranks(torch, world, dev, ms))
+    clk = clocks.stop() if clocks else None
+    plans["mixed"].check()
+    del plans["mixed"]
+    plans["fp64"] = BatchPlan(views, precision="fp64", inplace=True)
+    generate()
+    torch.cuda.synchronize()
+    t64 = _events_ms(torch, lambda: plans["fp64"].run(stream), stream)
+    plans["fp64"].check()
+    del plans, views, pool
+    torch.cuda.empty_cache()
+    # error on the 4-block sub-instance
+    e, _, b, sd = spec[0]
+    sub = workloads.tight_binding_device(4, b, e, sd, device=dev)
+    Gm = BatchPlan([sub], precision="mixed", digits=args.digits)
+    Gf = BatchPlan([sub])
+    Gm.run()
+    Gf.run()
+    Gm.check()
+    Gf.check()
+    dense = torch.zeros((4 * b, 4 * b), dtype=torch.complex128, device=dev)
+    d, u, l = sub
+    for i in range(4):
+        dense[i * b:(i + 1) * b, i * b:(i + 1) * b] = d[i]
+        if i < 3:
+            dense[i * b:(i + 1) * b, (i + 1) * b:(i + 2) * b] = u[i]
+            dense[(i + 1) * b:(i + 2) * b, i * b:(i + 1) * b] = l[i]
+    inv = torch.linalg.inv(dense)
+    ref_diag = torch.stack([inv[i * b:(i + 1) * b, i * b:(i + 1) * b] for i in range(4)])
+
+    def rel(a, r):
+        return float(torch.linalg.vector_norm(a - r) / torch.linalg.vector_norm(r))
+
+    err_fp64 = max(rel(a, r) for a, r in zip(Gm.results()[0], Gf.results()[0]) if r.numel())
+    err_dense = rel(Gm.results()[0][0], ref_diag)
+    ms = statistics.median(tm)
+    F = sum(workloads.rgf_flops(n, b) for (_, n, b, _) in spec)
+    return {"metric": "RGF matrices/s, n=256 b=1024 instances, mixed precision", "value": len(spec) * world / (ms * 1e-3),
+            "unit": "matrices/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128 (mixed products)",
+            "data": "synthetic",
+            "config": {"workload": "large_mixed_%dx(n=256,b=1024)" % len(spec), "count": len(spec),
+                       "input_gb": round(sum(in_elems(n, b) for (_, n, b, _) in spec) * 16 / 1e9, 1),
+                       "in_place": True, "digits": args.digits, "parallelism": "replicas%d" % world},
+            "gpu_launches": args.steps,
+            "fp64_same_wave": {"ms": t64, "matrices_per_s": len(spec) / (t64 * 1e-3), "mixed_over_fp64": t64 / ms},
+            "rel_err": {"mixed_vs_fp64_sub_instance": err_fp64, "mixed_diag_vs_dense_fp64_inverse": err_dense,
+                        "sub_instance": "n=4, b=1024, first instance's generator"},
+            "roofline": {"bound": "tensor", "achieved": F / (ms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s (FP64-equivalent)",
+                         "frac": F / (ms * 1e-3) / 1e12 / peak, "traffic": None, "kernel": "rgf_batched_kernel (mixed)",
+                         "flops": "canonical 8 b^3 (8(n-1)+n)", "peak_source": "sinvb_fp64_mma_peak (DMMA)"},
+            "clocks": clk}
+
+
+def reference_other(args, world):
+    """Reference arm of the non-default workloads (rank 0, host cores)."""
+    from sinv_b200 import workloads
+    from oracle import rgf_oracle
+    base = {"impl": "reference", "n_gpus": world, "steps": args.steps, "warmup": args.warmup}
+    if args.workload == "plain_large":
+        dn, un, ln = workloads.dominant(64, 256, seed=0)
+        ts = []
+        for _ in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            rgf_oracle.rgf(dn, un, ln)
+            ts.append(time.perf_counter() - t0)
+        v = 1.0 / statistics.median(ts)
+        base.update({"metric": "RGF matrices/s, one matrix, plain FP64 path", "value": v, "unit": "matrices/s",
+                     "higher_is_better": True, "config": {"workload": "plain_large(n=64,b=256)"},
+                     "cpu_baseline": {"value": v, "unit": "matrices/s", "cores": _blas_threads(), "kind": "port",
+                                      "sample": "the whole matrix per step"},
+                     "e2e": {"value": v, "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        return base
+    if args.workload == "large_mixed":
+        e, _, b, sd = workloads.large_mixed_spec(count=1)[0]
+        d, u, l = workloads.tight_binding(4, b, e, seed=sd)
+        t0 = time.perf_counter()
+        rgf_oracle.rgf(d, u, l)
+        t = (time.perf_counter() - t0) * workloads.rgf_flops(256, b) / workloads.rgf_flops(4, b)
+        v = 1.0 / t
+        base.update({"metric": "RGF matrices/s, n=256 b=1024 instances, mixed precision", "value": v,
+                     "unit": "matrices/s", "higher_is_better": True,
+                     "config": {"workload": "large_mixed(n=256,b=1024)"},
+                     "cpu_baseline": {"value": v, "unit": "matrices/s", "cores": _blas_threads(), "kind": "port",
+                                      "sample": "a 4-block sub-instance (n=4, b=1024) in FP64, extrapolated to "
+                                                "n=256 by the canonical flop count"},
+                     "e2e": {"value": v, "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        return base
+    base.update({"unavailable": "the reference computes no derivatives (no adjoint of rgf exists in it)"})
+    return base
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if not args.count:
+        args.count = {"energy_batch": 512, "gradient_set": 128, "large_mixed": 13, "plain_large": 1}[args.workload]
     if args.impl == "reference":
-        run_reference(args, rank, world)
+        if args.workload == "energy_batch":
+            run_reference(args, rank, world)
+        elif rank == 0:
+            print(json.dumps(reference_other(args, world)), flush=True)
         return
     import datetime
     import torch
@@ -477,7 +820,9 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
-        out = run_sinvb(args, rank, world, local_rank)
+        fn = {"energy_batch": run_sinvb, "plain_large": run_plain_large, "gradient_set": run_gradient_set,
+              "large_mixed": run_large_mixed}[args.workload]
+        out = fn(args, rank, world, local_rank)
         if rank == 0:
             print(json.dumps(out), flush=True)
     finally:

@@ -76,6 +76,42 @@ struct ItemArea {
 };
 static_assert(sizeof(ItemArea) == 64, "64-byte item areas");
 
+// Scratch slots are taken by a team's rank 0 from the bitmap hdr->slot_bits
+// (hdr->nslots slots, at least as many as teams that can run at once, so a
+// slot is normally free at once; the wait is bounded all the same).
+__device__ inline int acquire_scratch(WsHeader* hdr, int* status) {
+  const int K = (int)hdr->nslots;
+  unsigned long long t0 = 0;
+  for (unsigned spins = 0;; spins++) {
+    for (int w = 0; w * 32 < K; w++) {
+      const unsigned valid = (K - w * 32 >= 32) ? 0xffffffffu : ((1u << (K - w * 32)) - 1u);
+      unsigned cur = *((volatile unsigned*)&hdr->slot_bits[w]);
+      while (true) {
+        const unsigned freeb = ~cur & valid;
+        if (!freeb) break;
+        const int bit = __ffs(freeb) - 1;
+        const unsigned old = atomicOr(&hdr->slot_bits[w], 1u << bit);
+        if (!(old & (1u << bit))) return w * 32 + bit;
+        cur = old | (1u << bit);
+      }
+    }
+    __nanosleep(256);
+    if ((spins & 255) == 255) {
+      const unsigned long long now = global_ns();
+      if (t0 == 0) t0 = now;
+      else if (now - t0 > kTeamWaitNs) {
+        report(status, SINVB_STATUS_TIMEOUT);
+        return -1;
+      }
+    }
+  }
+}
+__device__ inline void release_scratch(WsHeader* hdr, int id) {
+  if (id < 0) return;
+  __threadfence();
+  atomicAnd(&hdr->slot_bits[id >> 5], ~(1u << (id & 31)));
+}
+
 // Persistent: every CTA repeatedly takes one queue slot.  Slot s belongs to the
 // instance k with slot_start[k] <= s < slot_start[k] + team[k], with rank
 // s - slot_start[k] in that instance's team.  Slots are handed out in order,
@@ -89,8 +125,6 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
   WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
   const BatchEntry<T>* entries = reinterpret_cast<const BatchEntry<T>*>(ws + hdr->desc_offset);
   ItemArea* items = reinterpret_cast<ItemArea*>(ws + hdr->items_offset);
-  if (blockIdx.x >= hdr->nslots) return;
-  unsigned char* my_slot = ws + hdr->slots_offset + (size_t)blockIdx.x * hdr->slot_bytes;
   const int count = hdr->count;
   const int total_slots = hdr->total_slots;
   const unsigned flags = hdr->flags;
@@ -117,13 +151,17 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
     const BatchEntry<T> e = entries[k];
     ItemArea* item = items + k;
     const int rank = s - e.slot_start;
+    __shared__ int sh_scratch;
     if (rank == 0 && threadIdx.x == 0) {
-      item->scratch = my_slot;
+      const int id = acquire_scratch(hdr, &item->status);
+      sh_scratch = id;
+      item->scratch = id < 0 ? nullptr : ws + hdr->slots_offset + (size_t)id * hdr->slot_bytes;
       __threadfence();
     }
     TeamDyn team{&item->counter, &item->status, rank, e.team, 0u};
     if (!team.sync()) continue;  // formation: the rank-0 scratch pointer is visible after this
     unsigned char* slot = *((unsigned char* volatile*)&item->scratch);
+    if (!slot) continue;  // no scratch slot came free (reported); the whole team skips
     const size_t bb = (size_t)e.b * e.b;
     RgfParams<T> p;
     p.diag = e.diag;
@@ -162,6 +200,9 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
       int st = *((volatile int*)&item->status);
       if (hdr->inst_status) hdr->inst_status[e.orig] = st;
       if (st) report(&hdr->status, st);
+      // the sweep ended on a team barrier, so no member touches the slot any
+      // more; after a failure members may still be running: keep it taken
+      if (!st) release_scratch(hdr, sh_scratch);
     }
   }
   if (Mixed) oz_teardown(&oz_state);
@@ -183,6 +224,29 @@ static unsigned batch_slots() {
   return (unsigned)device_sm_count();
 }
 
+static int team_size(int b, unsigned flags) {
+  if (flags & SINVB_FORCE_CTA) return 1;
+  if (b >= 1024) return 8;
+  if (b >= 512) return 4;
+  if (b >= 256) return 2;
+  return 1;
+}
+
+// Team of every instance: team_size(b), and when the default teams leave CTAs
+// of the grid idle (few instances), teams of b >= 256 grow to grid / count
+// CTAs, at most b / 64 (one 64-wide tile column each) and 16.
+static std::vector<int> batch_teams(const sinvb_batch_desc* d, int count, unsigned flags, int grid) {
+  std::vector<int> t(count);
+  long total = 0;
+  for (int k = 0; k < count; k++) total += t[k] = team_size(d[k].b, flags);
+  if (!(flags & SINVB_FORCE_CTA) && total < grid) {
+    const int share = grid / count;
+    for (int k = 0; k < count; k++)
+      if (d[k].b >= 256) t[k] = std::max(t[k], std::min({share, d[k].b / 64, 16}));
+  }
+  return t;
+}
+
 static BatchLayout batch_layout(const sinvb_batch_desc* d, int count, int dtype, unsigned flags) {
   BatchLayout L{};
   const size_t es = elem_bytes(dtype);
@@ -194,7 +258,10 @@ static BatchLayout batch_layout(const sinvb_batch_desc* d, int count, int dtype,
     if (mixed && d[k].b >= kMixedMinB) s += 2 * oz_op_scratch(d[k].b, d[k].b, d[k].b, mixed_digits(flags));
     slot = std::max(slot, s);
   }
-  L.nslots = batch_slots();
+  // scratch slots: as many as teams can run at once (grid / smallest team)
+  const std::vector<int> teams = batch_teams(d, count, flags, (int)batch_slots());
+  const int min_team = *std::min_element(teams.begin(), teams.end());
+  L.nslots = std::min<unsigned>(batch_slots() / min_team, 256u);
   L.desc_offset = sizeof(WsHeader);
   L.items_offset = align_up(L.desc_offset + (size_t)count * sizeof(BatchEntry<cplx>), 256);
   L.slots_offset = align_up(L.items_offset + (size_t)count * sizeof(ItemArea), 256);
@@ -224,13 +291,7 @@ static int check_batch(const sinvb_batch_desc* d, int count, unsigned flags, con
 }
 
 // CTAs per instance: enough tiles per CTA to stay busy, few enough barriers.
-static int team_size(int b, unsigned flags) {
-  if (flags & SINVB_FORCE_CTA) return 1;
-  if (b >= 1024) return 8;
-  if (b >= 512) return 4;
-  if (b >= 256) return 2;
-  return 1;
-}
+
 
 template <class T>
 static int launch_batched(void* ws, int count, unsigned flags, cudaStream_t stream) {
@@ -240,8 +301,10 @@ static int launch_batched(void* ws, int count, unsigned flags, cudaStream_t stre
   if (flags & SINVB_PREC_MIXED)
     smem = std::max(smem, std::max(oz_smem_bytes(mixed_digits(flags)), oz_slice_smem(mixed_digits(flags))));
   SINVB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  // reset status, barrier and queue, and every instance's team area
+  // reset status, barrier and queue, the scratch bitmap, and every instance's team area
   SINVB_CUDA(cudaMemsetAsync(ws, 0, 16, stream));
+  SINVB_CUDA(cudaMemsetAsync((unsigned char*)ws + offsetof(WsHeader, slot_bits), 0, sizeof(WsHeader::slot_bits),
+                             stream));
   const size_t items_offset = align_up(sizeof(WsHeader) + (size_t)count * sizeof(BatchEntry<cplx>), 256);
   SINVB_CUDA(cudaMemsetAsync((unsigned char*)ws + items_offset, 0, (size_t)count * sizeof(ItemArea), stream));
   unsigned char* w = (unsigned char*)ws;
@@ -258,6 +321,7 @@ static int upload_and_run(const sinvb_batch_desc* d, int count, unsigned flags, 
   int rc = check_batch(d, count, flags, ws, ws_bytes, dtype);
   if (rc) return rc;
   const BatchLayout L = batch_layout(d, count, dtype, flags);
+  const std::vector<int> teams = batch_teams(d, count, flags, (int)batch_slots());
   std::vector<BatchEntry<T>> entries(count);
   for (int k = 0; k < count; k++) {
     BatchEntry<T>& e = entries[k];
@@ -270,7 +334,7 @@ static int upload_and_run(const sinvb_batch_desc* d, int count, unsigned flags, 
     e.n = d[k].n;
     e.b = d[k].b;
     e.orig = k;
-    e.team = team_size(e.b, flags);
+    e.team = teams[k];
     e.slot_start = 0;
     e.pad[0] = e.pad[1] = e.pad[2] = 0;
   }

@@ -72,7 +72,7 @@ struct WsHeader {
   // batched launches: written by the upload, read by the persistent kernel
   int count;                  // instances
   unsigned int flags;
-  unsigned int nslots;        // per-CTA scratch slots
+  unsigned int nslots;        // scratch slots (batched: one per concurrent team)
   unsigned int pad0;
   unsigned long long slot_bytes;
   unsigned long long desc_offset;
@@ -80,7 +80,8 @@ struct WsHeader {
   int* inst_status;           // caller's per-instance status array (may be null)
   unsigned long long items_offset;
   int total_slots;            // sum of team sizes
-  unsigned int pad[45];
+  unsigned int slot_bits[8];  // batched: scratch slots in use (bit per slot, up to 256)
+  unsigned int pad[37];
 };
 static_assert(sizeof(WsHeader) == 256, "header is 256 bytes");
 
