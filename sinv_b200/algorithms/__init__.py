@@ -7,6 +7,6 @@ from . import rgf  # noqa: F401
 from . import bcr_serial  # noqa: F401
 from . import bcr_serial as bcr_s  # noqa: F401
 from . import batched  # noqa: F401
-from .batched import BatchPlan, rgf_batched  # noqa: F401
+from .batched import BatchPlan, rgf_batched, rgf_batched_host  # noqa: F401
 from . import adjoint  # noqa: F401
 from .adjoint import RGFFunction, rgf_autograd  # noqa: F401

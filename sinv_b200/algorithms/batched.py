@@ -30,6 +30,10 @@ class BatchPlan:
     ``team="cta"`` runs every instance on a single CTA; by default large
     blocks get teams of 2-8 CTAs.
 
+    ``workspace`` (optional): a device uint8 tensor to use instead of
+    allocating one when it is large enough (``workspace_bytes``); plans that
+    share one must run in order on one stream.
+
     ``precision="mixed"`` (complex128 only) computes the block products of
     both sweeps on the int8 tensor cores (Ozaki splitting into ``digits``
     int8 slices, exact int32 accumulation, FP64 reconstruction) and keeps
@@ -41,7 +45,7 @@ class BatchPlan:
     """
 
     def __init__(self, instances, sym_mat=False, save_off_diag=True, precision="fp64", outputs=None,
-                 device=None, inplace=False, team=None, digits=7):
+                 device=None, inplace=False, team=None, digits=7, workspace=None):
         torch = dev._torch()
         self.lib = _lib.load()
         if len(instances) == 0:
@@ -108,9 +112,29 @@ class BatchPlan:
         nbytes = self.lib.sinvb_rgf_batched_workspace_size(ctypes.cast(descs, ctypes.c_void_p), len(descs),
                                                            self.code, self.flags)
         with torch.cuda.device(self.device):
-            self.ws = dev.workspace(nbytes, self.device)
+            if workspace is not None and workspace.numel() >= nbytes and workspace.data_ptr() % 256 == 0:
+                self.ws = workspace  # shared with other plans run in order on one stream
+            else:
+                self.ws = dev.workspace(nbytes, self.device)
             self.status_dev = torch.zeros(len(descs), dtype=torch.int32, device=self.device)
         self.uploaded = False
+
+    @staticmethod
+    def workspace_bytes(shapes, dtype_code=None, flags=None, sym_mat=False, save_off_diag=True, precision="fp64",
+                        inplace=False, digits=7):
+        """Workspace bytes of a batch of (n, b) shapes (complex128 unless dtype_code)."""
+        lib = _lib.load()
+        code = _lib.C128 if dtype_code is None else dtype_code
+        if flags is None:
+            flags = (_lib.SYM if sym_mat else 0) | (_lib.SAVE_OFFDIAG if save_off_diag else 0)
+            if precision == "mixed":
+                flags |= _lib.PREC_MIXED | (int(digits) << _lib.PREC_DIGITS_SHIFT)
+            if inplace:
+                flags |= _lib.INPLACE
+        descs = (_lib.BatchDesc * len(shapes))()
+        for k, (n, b) in enumerate(shapes):
+            descs[k] = _lib.BatchDesc(None, None, None, None, None, None, int(n), int(b))
+        return int(lib.sinvb_rgf_batched_workspace_size(ctypes.cast(descs, ctypes.c_void_p), len(descs), code, flags))
 
     @property
     def count(self):
@@ -173,3 +197,96 @@ def rgf_batched(instances, sym_mat=False, save_off_diag=True, precision="fp64", 
     if check:
         plan.check()
     return plan.results(like=instances[0][0])
+
+
+def rgf_batched_host(instances, outputs=None, sym_mat=False, precision="fp64", digits=7, wave_bytes=None,
+                     device=None, check=True):
+    """Selected inversion of host-resident instances streamed through the GPU.
+
+    ``instances``: list of ``(A_diag, A_upper, A_lower)`` torch CPU tensors
+    (complex128 or float64; pinned memory lets the copies overlap the
+    compute).  ``outputs``: matching host tensors to receive
+    ``(G_diag, G_upper, G_lower)``; may be the inputs themselves (results over
+    the inputs); by default new host tensors.  Returns the outputs.
+
+    The batch is cut into waves of at most ``wave_bytes`` of input (default: a
+    quarter of the batch, at most a third of the free device memory), in their
+    given order.  Each wave runs as
+    one persistent launch, in place in one of two device buffers, while the
+    next wave's inputs copy in on one stream and the previous wave's results
+    copy out on another, so PCIe traffic hides behind the sweeps.  Off-diagonal
+    blocks are always computed.
+    """
+    torch = dev._torch()
+    device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    if not instances:
+        raise ValueError("empty batch")
+    tdt = instances[0][0].dtype
+    if tdt not in (torch.complex128, torch.float64):
+        raise TypeError("rgf_batched_host takes complex128 or float64 host tensors")
+    shapes = [(int(d.shape[0]), int(d.shape[1])) for d, _, _ in instances]
+    elems = [(3 * n - 2) * b * b for n, b in shapes]
+    esize = 16 if tdt == torch.complex128 else 8
+    if outputs is None:
+        outputs = [(torch.empty_like(d), torch.empty_like(u), torch.empty_like(l)) for d, u, l in instances]
+    with torch.cuda.device(device):
+        if wave_bytes is None:  # at least four waves, so copies overlap sweeps; two buffers fit
+            free, _ = torch.cuda.mem_get_info(device)
+            wave_bytes = max(min(free // 3, sum(elems) * esize // 4), max(elems) * esize, 1 << 30)
+        waves, cur, used = [], [], 0
+        for k, e in enumerate(elems):
+            if cur and (used + e) * esize > wave_bytes:
+                waves.append(cur)
+                cur, used = [], 0
+            cur.append(k)
+            used += e
+        waves.append(cur)
+        cap = max(sum(elems[k] for k in w) for w in waves)
+        bufs = [torch.empty(cap, dtype=tdt, device=device) for _ in range(min(2, len(waves)))]
+        ws_bytes = max(BatchPlan.workspace_bytes([shapes[k] for k in w], _lib.dtype_code(tdt), sym_mat=sym_mat,
+                                                 precision=precision, inplace=True, digits=digits) for w in waves)
+        ws = dev.workspace(ws_bytes, device)
+        s_in, s_run, s_out = torch.cuda.Stream(device), torch.cuda.Stream(device), torch.cuda.Stream(device)
+        out_done = [None] * len(waves)
+        plans = []
+        for wi, w in enumerate(waves):
+            buf = bufs[wi % len(bufs)]
+            views, off = [], 0
+            for k in w:
+                n, b = shapes[k]
+                parts = []
+                for rows in (n, n - 1, n - 1):
+                    parts.append(buf[off:off + rows * b * b].view(rows, b, b))
+                    off += rows * b * b
+                views.append(tuple(parts))
+            with torch.cuda.stream(s_in):
+                if wi >= 2:
+                    s_in.wait_event(out_done[wi - 2])  # the buffer's previous results are out
+                for k, v in zip(w, views):
+                    for dst, src in zip(v, instances[k]):
+                        if dst.numel():
+                            dst.copy_(src, non_blocking=True)
+                ev_in = torch.cuda.Event()
+                ev_in.record(s_in)
+            s_run.wait_event(ev_in)
+            with torch.cuda.stream(s_run):  # the plan's status array is cleared on the run stream
+                plan = BatchPlan(views, sym_mat=sym_mat, precision=precision, inplace=True, digits=digits,
+                                 workspace=ws)
+            plan.run(s_run)
+            ev_run = torch.cuda.Event()
+            ev_run.record(s_run)
+            plans.append(plan)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(ev_run)
+                for k, v in zip(w, views):
+                    for dst, src in zip(outputs[k], v):
+                        if src.numel():
+                            dst.copy_(src, non_blocking=True)
+                out_done[wi] = torch.cuda.Event()
+                out_done[wi].record(s_out)
+        s_out.synchronize()
+        s_run.synchronize()
+        if check:
+            for p in plans:
+                p.check()
+    return outputs
