@@ -210,8 +210,7 @@ def rgf_batched_host(instances, outputs=None, sym_mat=False, precision="fp64", d
     the inputs); by default new host tensors.  Returns the outputs.
 
     The batch is cut into waves of at most ``wave_bytes`` of input (default: a
-    quarter of the batch, at most a third of the free device memory), in their
-    given order.  Each wave runs as
+    third of the free device memory), in their given order.  Each wave runs as
     one persistent launch, in place in one of two device buffers, while the
     next wave's inputs copy in on one stream and the previous wave's results
     copy out on another, so PCIe traffic hides behind the sweeps.  Off-diagonal
@@ -230,9 +229,9 @@ def rgf_batched_host(instances, outputs=None, sym_mat=False, precision="fp64", d
     if outputs is None:
         outputs = [(torch.empty_like(d), torch.empty_like(u), torch.empty_like(l)) for d, u, l in instances]
     with torch.cuda.device(device):
-        if wave_bytes is None:  # at least four waves, so copies overlap sweeps; two buffers fit
+        if wave_bytes is None:  # as few waves as fit: each wave waits for its longest chain
             free, _ = torch.cuda.mem_get_info(device)
-            wave_bytes = max(min(free // 3, sum(elems) * esize // 4), max(elems) * esize, 1 << 30)
+            wave_bytes = max(free // 3, max(elems) * esize)
         waves, cur, used = [], [], 0
         for k, e in enumerate(elems):
             if cur and (used + e) * esize > wave_bytes:
