@@ -449,8 +449,10 @@ def e2e_streamed(torch, spec, args, dev, world):
 
     need = sum(in_elems(n, b) for (_, n, b, _) in spec) * 16
     idx = list(range(len(spec)))
-    if psutil.virtual_memory().available < 1.5 * need:
-        idx = list(range(0, len(spec), 4))
+    for stride in (2, 4, 8):  # whole batch, else every 2nd / 4th / 8th instance, as host memory allows
+        if psutil.virtual_memory().available >= 1.5 * sum(in_elems(spec[k][1], spec[k][2]) for k in idx) * 16:
+            break
+        idx = list(range(0, len(spec), stride))
     host = []
     for k in idx:
         _, n, b, _ = spec[k]
@@ -482,7 +484,8 @@ def e2e_streamed(torch, spec, args, dev, world):
     del host
     return {"value": len(idx) * world / statistics.median(times), "unit": UNIT,
             "h2d_bytes_per_step": bytes_step, "d2h_bytes_per_step": bytes_step,
-            "sample": ("the whole batch" if len(idx) == len(spec) else "every 4th instance (%d)" % len(idx))
+            "sample": ("the whole batch" if len(idx) == len(spec) else
+                       "every %dth instance (%d)" % (len(spec) // len(idx), len(idx)))
                       + ", %.0f GB each way through pinned host memory; rgf_batched_host overlaps the copies "
                         "of one wave with the sweeps of another; wall clock around the call" % (bytes_step / 1e9)}
 

@@ -185,6 +185,24 @@ int sinvb_rgf_batched_z(const sinvb_batch_desc* descs, int count, unsigned flags
 int sinvb_rgf_batched_d(const sinvb_batch_desc* descs, int count, unsigned flags, void* workspace,
                         size_t workspace_bytes, int* status, sinvb_stream_t stream);
 /*
+ * Streamed form of the batched call, for inputs still arriving from the host:
+ * instance k (index into ``descs``) starts only once the device word
+ * ``ready[k]`` equals ``gen`` (the caller's copy stream writes it after the
+ * instance's inputs, in stream order), and on finishing the kernel sets
+ * ``done[k] = gen`` (system scope) so the caller can start copying its
+ * results out while the launch runs on.  Waits are bounded (status
+ * SINVB_STATUS_TIMEOUT).  ``gen`` must differ from every value the two
+ * arrays held before (a call counter); ``ready`` / ``done``: ``count``
+ * device words each.  Instances are taken largest b^3 n first, so the caller
+ * should copy them in that order.
+ */
+int sinvb_rgf_batched_stream_z(const sinvb_batch_desc* descs, int count, unsigned flags, void* workspace,
+                               size_t workspace_bytes, int* status, const unsigned* ready, unsigned* done,
+                               unsigned gen, sinvb_stream_t stream);
+int sinvb_rgf_batched_stream_d(const sinvb_batch_desc* descs, int count, unsigned flags, void* workspace,
+                               size_t workspace_bytes, int* status, const unsigned* ready, unsigned* done,
+                               unsigned gen, sinvb_stream_t stream);
+/*
  * Re-runs the batch last uploaded into ``workspace`` (same descriptors, same
  * buffers) with no host-to-device traffic: one memset and one kernel launch,
  * suitable for stream capture into a CUDA graph.

@@ -48,6 +48,8 @@ SIGNATURES = {
     "sinvb_rgf_batched_workspace_size": (_sz, [_vp, _i, _i, _u]),
     "sinvb_rgf_batched_z": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp]),
     "sinvb_rgf_batched_d": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp]),
+    "sinvb_rgf_batched_stream_z": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp, _vp, _u, _vp]),
+    "sinvb_rgf_batched_stream_d": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp, _vp, _u, _vp]),
     "sinvb_rgf_batched_rerun_z": (_i, [_vp, _vp]),
     "sinvb_rgf_batched_rerun_d": (_i, [_vp, _vp]),
     "sinvb_rgf_z_noalloc": (_i, [_vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _vp]),

@@ -156,6 +156,20 @@ class BatchPlan:
                     self.lib.sinvb_rgf_batched_rerun_d
                 _lib.check(fn(dev.ptr(self.ws), h), "sinvb_rgf_batched_rerun")
 
+    def run_streamed(self, ready, done, gen, stream=None):
+        """Enqueue the batch so that instance k waits for ``ready[k] == gen``
+        and raises ``done[k] = gen`` when finished (device int32 tensors of
+        ``count`` words; see ``sinvb_rgf_batched_stream_z``).  Uploads the
+        descriptors again on every call."""
+        torch = dev._torch()
+        with torch.cuda.device(self.device):
+            fn = self.lib.sinvb_rgf_batched_stream_z if self.code == _lib.C128 else self.lib.sinvb_rgf_batched_stream_d
+            rc = fn(ctypes.cast(self.descs, ctypes.c_void_p), len(self.descs), self.flags, dev.ptr(self.ws),
+                    self.ws.numel(), dev.ptr(self.status_dev), dev.ptr(ready), dev.ptr(done), int(gen),
+                    dev.stream_handle(stream))
+            _lib.check(rc, "sinvb_rgf_batched_stream")
+            self.uploaded = True
+
     def statuses(self):
         """Per-instance device status (synchronises)."""
         return self.status_dev.cpu().numpy()
@@ -221,6 +235,12 @@ def rgf_batched_host(instances, outputs=None, sym_mat=False, precision="fp64", d
     if not instances:
         raise ValueError("empty batch")
     tdt = instances[0][0].dtype
+    if wave_bytes is None:
+        free, _ = torch.cuda.mem_get_info(device)
+        esize_ = 16 if tdt == torch.complex128 else 8
+        total = sum((3 * int(d.shape[0]) - 2) * int(d.shape[1]) ** 2 for d, _, _ in instances) * esize_
+        if total + (8 << 30) <= free:  # the whole batch fits: one launch, copies overlapping it
+            return _host_one_launch(torch, instances, outputs, sym_mat, precision, digits, device, check)
     if tdt not in (torch.complex128, torch.float64):
         raise TypeError("rgf_batched_host takes complex128 or float64 host tensors")
     shapes = [(int(d.shape[0]), int(d.shape[1])) for d, _, _ in instances]
@@ -288,4 +308,78 @@ def rgf_batched_host(instances, outputs=None, sym_mat=False, precision="fp64", d
         if check:
             for p in plans:
                 p.check()
+    return outputs
+
+
+_gen_counter = [0]
+
+
+def _host_one_launch(torch, instances, outputs, sym_mat, precision, digits, device, check):
+    """rgf_batched_host when the whole batch fits on the device: one persistent
+    launch whose teams wait for each instance's inputs (ready flags written
+    after its copies) while the host copies them in, largest b^3 n first (the
+    kernel's order); the host polls the done flags and copies each finished
+    instance out while the launch runs on."""
+    tdt = instances[0][0].dtype
+    shapes = [(int(d.shape[0]), int(d.shape[1])) for d, _, _ in instances]
+    if outputs is None:
+        outputs = [(torch.empty_like(d), torch.empty_like(u), torch.empty_like(l)) for d, u, l in instances]
+    order = sorted(range(len(shapes)), key=lambda k: -(shapes[k][1] ** 3) * shapes[k][0])  # stable, as the kernel
+    _gen_counter[0] += 1
+    gen = _gen_counter[0]
+    with torch.cuda.device(device):
+        buf = torch.empty(sum((3 * n - 2) * b * b for n, b in shapes), dtype=tdt, device=device)
+        views, off = [None] * len(shapes), 0
+        for k, (n, b) in enumerate(shapes):
+            parts = []
+            for rows in (n, n - 1, n - 1):
+                parts.append(buf[off:off + rows * b * b].view(rows, b, b))
+                off += rows * b * b
+            views[k] = tuple(parts)
+        count = len(shapes)
+        ready = torch.zeros(count, dtype=torch.int32, device=device)
+        done = torch.zeros(count, dtype=torch.int32, device=device)
+        gen_host = torch.full((1,), gen, dtype=torch.int32).pin_memory()
+        done_host = torch.zeros(count, dtype=torch.int32).pin_memory()
+        s_in, s_run, s_out, s_poll = (torch.cuda.Stream(device) for _ in range(4))
+        init = torch.cuda.Event()
+        init.record(torch.cuda.current_stream(device))  # buffers and flag arrays allocated and zeroed
+        for s_ in (s_in, s_run, s_out, s_poll):
+            s_.wait_event(init)
+        with torch.cuda.stream(s_run):
+            plan = BatchPlan(views, sym_mat=sym_mat, precision=precision, inplace=True, digits=digits)
+        plan.run_streamed(ready, done, gen, s_run)
+        with torch.cuda.stream(s_in):
+            for k in order:
+                for dst, src in zip(views[k], instances[k]):
+                    if dst.numel():
+                        dst.copy_(src, non_blocking=True)
+                ready[k:k + 1].copy_(gen_host, non_blocking=True)
+        issued = [False] * count
+        left = count
+        import time as _time
+        t_start = _time.monotonic()
+        while left:
+            with torch.cuda.stream(s_poll):
+                done_host.copy_(done, non_blocking=True)
+            s_poll.synchronize()
+            flags_now = done_host.numpy()
+            kernel_over = s_run.query()
+            for k in order:
+                if not issued[k] and (flags_now[k] == gen or kernel_over):
+                    with torch.cuda.stream(s_out):
+                        for dst, src in zip(outputs[k], views[k]):
+                            if src.numel():
+                                dst.copy_(src, non_blocking=True)
+                    issued[k] = True
+                    left -= 1
+            if left and _time.monotonic() - t_start > 3600:
+                raise RuntimeError("rgf_batched_host: instances never finished")
+            if left:
+                _time.sleep(0.0005)
+        s_out.synchronize()
+        s_run.synchronize()
+        if check:
+            plan.check()
+        del buf
     return outputs

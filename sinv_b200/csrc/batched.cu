@@ -106,6 +106,34 @@ __device__ inline int acquire_scratch(WsHeader* hdr, int* status) {
     }
   }
 }
+// Streamed batches: the inputs of instance k are in place once ready[k]
+// holds this call's generation (written by a copy after the data, in stream
+// order); a bounded wait, reported as a timeout.
+__device__ inline void wait_ready(const WsHeader* hdr, int k, int* status) {
+  const unsigned gen = hdr->gen;
+  unsigned long long t0 = 0;
+  for (unsigned spins = 0;; spins++) {
+    unsigned v;
+    asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(hdr->ready + k) : "memory");
+    if (v == gen) return;
+    __nanosleep(512);
+    if ((spins & 255) == 255) {
+      const unsigned long long now = global_ns();
+      if (t0 == 0) t0 = now;
+      else if (now - t0 > kTeamWaitNs) {
+        report(status, SINVB_STATUS_TIMEOUT);
+        return;
+      }
+    }
+  }
+}
+// ... and done[k] tells the host that instance k's results may be copied out.
+__device__ inline void signal_done(const WsHeader* hdr, int k) {
+  if (!hdr->done) return;
+  __threadfence_system();
+  asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(hdr->done + k), "r"(hdr->gen) : "memory");
+}
+
 __device__ inline void release_scratch(WsHeader* hdr, int id) {
   if (id < 0) return;
   __threadfence();
@@ -153,15 +181,22 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
     const int rank = s - e.slot_start;
     __shared__ int sh_scratch;
     if (rank == 0 && threadIdx.x == 0) {
+      if (hdr->ready) wait_ready(hdr, e.orig, &item->status);
       const int id = acquire_scratch(hdr, &item->status);
       sh_scratch = id;
       item->scratch = id < 0 ? nullptr : ws + hdr->slots_offset + (size_t)id * hdr->slot_bytes;
       __threadfence();
     }
     TeamDyn team{&item->counter, &item->status, rank, e.team, 0u};
-    if (!team.sync()) continue;  // formation: the rank-0 scratch pointer is visible after this
+    if (!team.sync()) {  // formation: the rank-0 scratch pointer is visible after this
+      if (rank == 0 && threadIdx.x == 0) signal_done(hdr, e.orig);
+      continue;
+    }
     unsigned char* slot = *((unsigned char* volatile*)&item->scratch);
-    if (!slot) continue;  // no scratch slot came free (reported); the whole team skips
+    if (!slot) {  // no scratch slot came free (reported); the whole team skips
+      if (rank == 0 && threadIdx.x == 0) signal_done(hdr, e.orig);
+      continue;
+    }
     const size_t bb = (size_t)e.b * e.b;
     RgfParams<T> p;
     p.diag = e.diag;
@@ -203,6 +238,7 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
       // the sweep ended on a team barrier, so no member touches the slot any
       // more; after a failure members may still be running: keep it taken
       if (!st) release_scratch(hdr, sh_scratch);
+      signal_done(hdr, e.orig);
     }
   }
   if (Mixed) oz_teardown(&oz_state);
@@ -317,7 +353,8 @@ static int launch_batched(void* ws, int count, unsigned flags, cudaStream_t stre
 
 template <class T>
 static int upload_and_run(const sinvb_batch_desc* d, int count, unsigned flags, void* ws, size_t ws_bytes,
-                          int* status, cudaStream_t stream, int dtype) {
+                          int* status, cudaStream_t stream, int dtype, const unsigned* ready = nullptr,
+                          unsigned* done = nullptr, unsigned gen = 0) {
   int rc = check_batch(d, count, flags, ws, ws_bytes, dtype);
   if (rc) return rc;
   const BatchLayout L = batch_layout(d, count, dtype, flags);
@@ -357,6 +394,9 @@ static int upload_and_run(const sinvb_batch_desc* d, int count, unsigned flags, 
   h.inst_status = status;
   h.items_offset = L.items_offset;
   h.total_slots = total_slots;
+  h.ready = ready;
+  h.done = done;
+  h.gen = gen;
   unsigned char* w = (unsigned char*)ws;
   SINVB_CUDA(cudaMemcpyAsync(w, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
   SINVB_CUDA(cudaMemcpyAsync(w + L.desc_offset, entries.data(), count * sizeof(BatchEntry<T>),
@@ -411,6 +451,24 @@ int sinvb_rgf_batched_d(const sinvb_batch_desc* descs, int count, unsigned flags
   if (flags & SINVB_PREC_MIXED) return SINVB_EUNSUPPORTED;
   return upload_and_run<double>(descs, count, flags, workspace, workspace_bytes, status, (cudaStream_t)stream,
                                 SINVB_F64);
+}
+
+int sinvb_rgf_batched_stream_z(const sinvb_batch_desc* descs, int count, unsigned flags, void* workspace,
+                               size_t workspace_bytes, int* status, const unsigned* ready, unsigned* done,
+                               unsigned gen, sinvb_stream_t stream) {
+  if (!ready || !done || gen == 0) return SINVB_EINVAL;
+  if ((flags & SINVB_PREC_MIXED) && mixed_digits(flags) > kOzMaxDigits) return SINVB_EINVAL;
+  return upload_and_run<cplx>(descs, count, flags, workspace, workspace_bytes, status, (cudaStream_t)stream,
+                              SINVB_C128, ready, done, gen);
+}
+
+int sinvb_rgf_batched_stream_d(const sinvb_batch_desc* descs, int count, unsigned flags, void* workspace,
+                               size_t workspace_bytes, int* status, const unsigned* ready, unsigned* done,
+                               unsigned gen, sinvb_stream_t stream) {
+  if (!ready || !done || gen == 0) return SINVB_EINVAL;
+  if (flags & SINVB_PREC_MIXED) return SINVB_EUNSUPPORTED;
+  return upload_and_run<double>(descs, count, flags, workspace, workspace_bytes, status, (cudaStream_t)stream,
+                                SINVB_F64, ready, done, gen);
 }
 
 int sinvb_rgf_batched_rerun_z(void* workspace, sinvb_stream_t stream) {

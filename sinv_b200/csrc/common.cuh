@@ -81,7 +81,10 @@ struct WsHeader {
   unsigned long long items_offset;
   int total_slots;            // sum of team sizes
   unsigned int slot_bits[8];  // batched: scratch slots in use (bit per slot, up to 256)
-  unsigned int pad[37];
+  const unsigned int* ready;  // batched, streamed: instance k starts once ready[k] == gen
+  unsigned int* done;         // batched, streamed: done[k] = gen when instance k has finished
+  unsigned int gen;
+  unsigned int pad[30];
 };
 static_assert(sizeof(WsHeader) == 256, "header is 256 bytes");
 

@@ -124,17 +124,20 @@ def test_teams_for_large_blocks_and_in_place(inplace):
             assert _rel(a.cpu().numpy(), b.cpu().numpy()) <= 1e-12
 
 
+@pytest.mark.parametrize("wave_bytes", [6 * 2 ** 20, None])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_host_streamed_batch_matches_device_batch(precision):
-    """rgf_batched_host: waves of a few instances (buffer reuse across waves),
-    copies on their own streams, results written over the host inputs."""
+def test_host_streamed_batch_matches_device_batch(precision, wave_bytes):
+    """rgf_batched_host, results written over the host inputs: waves of a few
+    instances (buffer reuse across waves), or (wave_bytes=None, the batch fits)
+    one launch whose teams wait for each instance's copy-in flag while the
+    host copies out finished instances."""
     import torch
     from sinv_b200.algorithms import rgf_batched_host
     shapes = [(3, 256), (5, 64), (2, 130), (4, 32), (3, 300), (6, 16), (2, 64)]
     inst = [workloads.tight_binding(n, b, 0.2 + 0.05 * k, seed=600 + k) for k, (n, b) in enumerate(shapes)]
     host = [tuple(torch.from_numpy(x.copy()).pin_memory() for x in t) for t in inst]
     ref = rgf_batched(inst, precision=precision)
-    out = rgf_batched_host(host, outputs=host, precision=precision, wave_bytes=6 * 2 ** 20)
+    out = rgf_batched_host(host, outputs=host, precision=precision, wave_bytes=wave_bytes)
     assert out is host
     for (d, u, l), G, R in zip(inst, out, ref):
         for g, r in zip(G, R):
