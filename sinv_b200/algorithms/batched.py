@@ -156,6 +156,22 @@ class BatchPlan:
                     self.lib.sinvb_rgf_batched_rerun_d
                 _lib.check(fn(dev.ptr(self.ws), h), "sinvb_rgf_batched_rerun")
 
+    def capture(self):
+        """A ``torch.cuda.CUDAGraph`` holding one re-run of this batch (the
+        workspace memsets and the persistent launch).  Replaying it recomputes
+        every instance from the current contents of the input tensors; the
+        first call uploads the descriptors outside the graph."""
+        torch = dev._torch()
+        with torch.cuda.device(self.device):
+            if not self.uploaded:
+                self.run()
+            torch.cuda.synchronize(self.device)
+            g = torch.cuda.CUDAGraph()
+            s = torch.cuda.Stream(self.device)
+            with torch.cuda.graph(g, stream=s):
+                self.run(s)
+            return g
+
     def run_streamed(self, ready, done, gen, stream=None):
         """Enqueue the batch so that instance k waits for ``ready[k] == gen``
         and raises ``done[k] = gen`` when finished (device int32 tensors of

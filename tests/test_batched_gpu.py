@@ -143,3 +143,38 @@ def test_host_streamed_batch_matches_device_batch(precision, wave_bytes):
         for g, r in zip(G, R):
             if r.size:
                 assert _rel(g.numpy(), r) <= 1e-12, _rel(g.numpy(), r)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_rerun_captured_in_cuda_graph(precision):
+    """BatchPlan.capture(): the re-run (memsets + persistent cooperative launch)
+    as a CUDA graph; replays reproduce the eager results bit for bit and follow
+    new input values."""
+    import torch
+    shapes = [(4, 256), (3, 64), (5, 32), (2, 300)]
+    inst = [workloads.tight_binding(n, b, 0.1 * k, seed=700 + k) for k, (n, b) in enumerate(shapes)]
+    tinst = [tuple(torch.from_numpy(x).cuda() for x in t) for t in inst]
+    plan = BatchPlan(tinst, precision=precision)
+    plan.run()
+    plan.check()
+    eager = [tuple(g.clone() for g in G) for G in plan.results()]
+    graph = plan.capture()
+    for G in plan.results():
+        for g in G:
+            g.zero_()
+    graph.replay()
+    graph.replay()
+    torch.cuda.synchronize()
+    plan.check()
+    for G0, G1 in zip(eager, plan.results()):
+        for a, b in zip(G0, G1):
+            assert torch.equal(a, b)
+    # new inputs in the same tensors: the replay follows them
+    new = workloads.tight_binding(4, 256, 0.55, seed=777)
+    for dst, src in zip(tinst[0], new):
+        dst.copy_(torch.from_numpy(src))
+    graph.replay()
+    torch.cuda.synchronize()
+    ref = rgf_batched([new], precision=precision)[0]
+    for g, r in zip(plan.results()[0], ref):
+        assert _rel(g.cpu().numpy(), r) <= 1e-12
