@@ -229,6 +229,13 @@ def rgf_batched(instances, sym_mat=False, save_off_diag=True, precision="fp64", 
     return plan.results(like=instances[0][0])
 
 
+def _available_bytes(torch, device):
+    """Device bytes a new allocation can get: free memory plus the blocks
+    torch's caching allocator holds but no tensor uses."""
+    free, _ = torch.cuda.mem_get_info(device)
+    return free + torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
+
+
 def rgf_batched_host(instances, outputs=None, sym_mat=False, precision="fp64", digits=7, wave_bytes=None,
                      device=None, check=True):
     """Selected inversion of host-resident instances streamed through the GPU.
@@ -252,7 +259,7 @@ def rgf_batched_host(instances, outputs=None, sym_mat=False, precision="fp64", d
         raise ValueError("empty batch")
     tdt = instances[0][0].dtype
     if wave_bytes is None:
-        free, _ = torch.cuda.mem_get_info(device)
+        free = _available_bytes(torch, device)
         esize_ = 16 if tdt == torch.complex128 else 8
         total = sum((3 * int(d.shape[0]) - 2) * int(d.shape[1]) ** 2 for d, _, _ in instances) * esize_
         if total + (8 << 30) <= free:  # the whole batch fits: one launch, copies overlapping it
@@ -266,7 +273,7 @@ def rgf_batched_host(instances, outputs=None, sym_mat=False, precision="fp64", d
         outputs = [(torch.empty_like(d), torch.empty_like(u), torch.empty_like(l)) for d, u, l in instances]
     with torch.cuda.device(device):
         if wave_bytes is None:  # as few waves as fit: each wave waits for its longest chain
-            free, _ = torch.cuda.mem_get_info(device)
+            free = _available_bytes(torch, device)
             wave_bytes = max(free // 3, max(elems) * esize)
         waves, cur, used = [], [], 0
         for k, e in enumerate(elems):
