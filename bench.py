@@ -575,7 +575,7 @@ def run_plain_large(args, rank, world, local_rank):
     is one selected inversion; every rank inverts its own copy (replicas)."""
     import torch
     from sinv_b200 import workloads
-    from sinv_b200.algorithms import bcr_s, rgf
+    from sinv_b200.algorithms import bcr_s, rgf, rgf2s
     from oracle import rgf_oracle
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
@@ -586,7 +586,7 @@ def run_plain_large(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MB > L2
     clocks = Clocks(local_rank) if rank == 0 else None
-    ts, tb = [], []
+    ts, tb, t2 = [], [], []
     for step in range(args.warmup + args.steps):
         if step == args.warmup and clocks:
             clocks.start()
@@ -594,9 +594,12 @@ def run_plain_large(args, rank, world, local_rank):
         ms = _events_ms(torch, lambda: rgf.rgf_blocks(d, u, l, check=False), stream)
         flush.zero_()
         mb = _events_ms(torch, lambda: bcr_s.bcr_blocks(d, u, l, check=False), stream)
+        flush.zero_()
+        m2 = _events_ms(torch, lambda: rgf2s.rgf2sided(d, u, l, check=False), stream)
         if step >= args.warmup:
             ts.append(_max_over_ranks(torch, world, dev, ms))
             tb.append(_max_over_ranks(torch, world, dev, mb))
+            t2.append(_max_over_ranks(torch, world, dev, m2))
     clk = clocks.stop() if clocks else None
     G = rgf.rgf_blocks(d, u, l)
     R = rgf_oracle.rgf(dn, un, ln)
@@ -627,6 +630,9 @@ def run_plain_large(args, rank, world, local_rank):
                         "frac": F / (ms * 1e-3) / 1e12 / peak, "traffic": None, "kernel": "rgf_grid_kernel",
                         "flops": "canonical 8 b^3 (8(n-1)+n)", "peak_source": "sinvb_fp64_mma_peak (DMMA)"},
            "bcr": {"ms": statistics.median(tb), "matrices_per_s": world / (statistics.median(tb) * 1e-3)},
+           "rgf2sided": {"ms": statistics.median(t2), "matrices_per_s": world / (statistics.median(t2) * 1e-3),
+                         "rel_err_vs_oracle": max(float(np.linalg.norm(g.cpu().numpy() - r) / np.linalg.norm(r))
+                                                  for g, r in zip(rgf2s.rgf2sided(d, u, l), R))},
            "clocks": clk,
            "e2e": {"value": world / (statistics.median(te) * 1e-3), "unit": "matrices/s",
                    "h2d_bytes_per_step": bytes_in, "d2h_bytes_per_step": bytes_in}}

@@ -94,6 +94,23 @@ int sinvb_rgf_s(const void* diag, const void* upper, const void* lower, int n, i
                 void* workspace, size_t workspace_bytes, sinvb_stream_t stream);
 
 /*
+ * Two-sided RGF on one GPU.  Replaces ``rgf2sided(A_diag, A_upper, A_lower,
+ * sym_mat, save_off_diag)`` of src/sinv/algorithms/rgf/rgf2sided.py:18-274
+ * (two MPI processes sweeping towards the middle) with two teams of CTAs of
+ * one launch: the dependency chain of a single matrix is about n/2 block
+ * steps instead of n.  Same arrays and results as sinvb_rgf_*; requires
+ * SINVB_SAVE_OFFDIAG (the halves keep their X / P blocks in G_upper and
+ * G_lower); SINVB_SYM allowed; complex128 and float64.
+ */
+size_t sinvb_rgf2s_workspace_size(int n, int b, int dtype, unsigned flags);
+int sinvb_rgf2s_z(const void* diag, const void* upper, const void* lower, int n, int b,
+                  unsigned flags, void* G_diag, void* G_upper, void* G_lower,
+                  void* workspace, size_t workspace_bytes, sinvb_stream_t stream);
+int sinvb_rgf2s_d(const void* diag, const void* upper, const void* lower, int n, int b,
+                  unsigned flags, void* G_diag, void* G_upper, void* G_lower,
+                  void* workspace, size_t workspace_bytes, sinvb_stream_t stream);
+
+/*
  * Device status word of a workspace: synchronises ``stream`` and returns the
  * status (SINVB_OK or a positive SINVB_STATUS_*) in *status.  The word is
  * reset by the next call that uses the workspace.

@@ -1,9 +1,12 @@
 """Selected-inversion algorithms, mirroring ``sinv.algorithms``
 (``src/sinv/algorithms/__init__.py:3-9``): ``rgf`` is the RGF module
-(``rgf.rgf(...)``) and ``bcr_s`` the BCR module (``bcr_s.bcr_serial(...)``).  The MPI-distributed algorithms of the reference
-(rgf2sided, bcr_parallel, psr, pdiv) are not part of this library."""
+(``rgf.rgf(...)``) and ``bcr_s`` the BCR module (``bcr_s.bcr_serial(...)``).  ``rgf2s`` is the two-sided RGF
+(``rgf2s.rgf2sided(...)``), both halves on one GPU.  The MPI-distributed
+algorithms of the reference (bcr_parallel, psr, pdiv) are not part of this
+library."""
 
 from . import rgf  # noqa: F401
+from . import rgf2sided as rgf2s  # noqa: F401
 from . import bcr_serial  # noqa: F401
 from . import bcr_serial as bcr_s  # noqa: F401
 from . import batched  # noqa: F401

@@ -84,7 +84,8 @@ struct WsHeader {
   const unsigned int* ready;  // batched, streamed: instance k starts once ready[k] == gen
   unsigned int* done;         // batched, streamed: done[k] = gen when instance k has finished
   unsigned int gen;
-  unsigned int pad[30];
+  unsigned int barrier_half[2];  // two-sided RGF: the left and right teams' barrier counters
+  unsigned int pad[28];
 };
 static_assert(sizeof(WsHeader) == 256, "header is 256 bytes");
 
