@@ -117,6 +117,21 @@ int sinvb_rgf2s_d(const void* diag, const void* upper, const void* lower, int n,
  */
 int sinvb_workspace_status(const void* workspace, sinvb_stream_t stream, int* status);
 
+/* ---- lesser Green's function ------------------------------------------------- */
+/*
+ * No reference counterpart: the step a transport code takes after rgf
+ * (src/sinv/algorithms/rgf/rgf.py:17-64) at each energy, G< = G Sigma< G^H on
+ * the tridiagonal blocks for a block-diagonal lesser self-energy
+ * (``sigma_lesser``: n blocks).  Writes the retarded blocks as sinvb_rgf_z
+ * with SAVE_OFFDIAG, and GL_diag (n blocks G<_ii), GL_upper (n-1 blocks
+ * G<_{i,i+1}); G<_{i+1,i} = -(G<_{i,i+1})^H.  complex128; flags: FORCE_CTA or
+ * FORCE_GRID only.
+ */
+size_t sinvb_rgf_lesser_workspace_size(int n, int b);
+int sinvb_rgf_lesser_z(const void* diag, const void* upper, const void* lower, const void* sigma_lesser, int n,
+                       int b, unsigned flags, void* G_diag, void* G_upper, void* G_lower, void* GL_diag,
+                       void* GL_upper, void* workspace, size_t workspace_bytes, sinvb_stream_t stream);
+
 /* ---- adjoint (reverse mode) of the RGF sweeps ------------------------------------ */
 /*
  * No reference counterpart (the reference has no gradients); the adjoint of

@@ -49,6 +49,8 @@ SIGNATURES = {
     "sinvb_rgf2s_workspace_size": (_sz, [_i, _i, _i, _u]),
     "sinvb_rgf2s_z": (_i, [_vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _sz, _vp]),
     "sinvb_rgf2s_d": (_i, [_vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "sinvb_rgf_lesser_workspace_size": (_sz, [_i, _i]),
+    "sinvb_rgf_lesser_z": (_i, [_vp, _vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "sinvb_rgf_batched_z": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp]),
     "sinvb_rgf_batched_d": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp]),
     "sinvb_rgf_batched_stream_z": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp, _vp, _u, _vp]),

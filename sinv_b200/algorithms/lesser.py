@@ -1,0 +1,46 @@
+"""Lesser Green's function on the tridiagonal blocks: G< = G Sigma< G^H.
+
+No reference counterpart: in a transport code this is the step after ``rgf``
+(``src/sinv/algorithms/rgf/rgf.py:17-64``) at every energy point, with the
+lesser self-energy Sigma< of the contacts (block-diagonal).  One sweep pair
+(``sinvb_rgf_lesser_z``) gives the retarded blocks of ``rgf`` and the lesser
+blocks G<_ii, G<_{i,i+1}; G<_{i+1,i} = -(G<_{i,i+1})^H (G< is anti-Hermitian).
+"""
+
+import numpy as np
+
+from .. import _lib
+from . import _device as dev
+
+
+def rgf_lesser(A_diag, A_upper, A_lower, Sigma_lesser, team=None, check=True, stream=None):
+    """``(A blocks, Sigma<_ii blocks) -> (G_diag, G_upper, G_lower, GL_diag, GL_upper, GL_lower)``.
+
+    complex128, numpy or torch (numpy in, numpy out).  ``Sigma_lesser``: (n, b, b).
+    ``team``: ``"cta"`` or ``"grid"`` as for ``rgf.rgf_blocks``.
+    """
+    torch = dev._torch()
+    lib = _lib.load()
+    tdt = dev.torch_dtype(A_diag)
+    if tdt != torch.complex128:
+        raise TypeError("rgf_lesser takes complex128 blocks")
+    d = dev.to_device(A_diag, tdt)
+    n, b = int(d.shape[0]), int(d.shape[1])
+    s = dev.to_device(Sigma_lesser, tdt)
+    if tuple(s.shape) != (n, b, b):
+        raise ValueError("Sigma_lesser must be (%d, %d, %d)" % (n, b, b))
+    u = dev.to_device(A_upper, tdt) if n > 1 else None
+    l = dev.to_device(A_lower, tdt) if n > 1 else None
+    flags = {None: 0, "cta": _lib.FORCE_CTA, "grid": _lib.FORCE_GRID}[team]
+    out = [torch.empty((k, b, b), dtype=tdt, device=d.device) for k in (n, n - 1, n - 1, n, n - 1)]
+    with torch.cuda.device(d.device):
+        ws = dev.workspace(lib.sinvb_rgf_lesser_workspace_size(n, b), d.device)
+        rc = lib.sinvb_rgf_lesser_z(dev.ptr(d), dev.ptr(u), dev.ptr(l), dev.ptr(s), n, b, flags,
+                                    *(dev.ptr(t) if t.numel() else None for t in out), dev.ptr(ws), ws.numel(),
+                                    dev.stream_handle(stream))
+        _lib.check(rc, "sinvb_rgf_lesser")
+        if check:
+            dev.raise_for_status(dev.read_status(lib, ws, stream), "rgf_lesser")
+    Gd, Gu, Gl, GLd, GLu = out
+    GLl = -GLu.conj().transpose(1, 2).contiguous()
+    return tuple(dev.to_output(t, A_diag) for t in (Gd, Gu, Gl, GLd, GLu, GLl))
