@@ -12,14 +12,16 @@ larger than L2 (126 MB) in every wave.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sinvb|reference]
                     [--precision mixed|fp64] [--count 512]
-                    [--workload energy_batch|plain_large|gradient_set|large_mixed]
+                    [--workload energy_batch|plain_large|gradient_set|large_mixed|bcr_batch]
 
 The default workload is the energy batch in mixed precision (block products
 on the int8 tensor cores for b >= 256, FP64 inverses).  The other workloads:
 plain_large (one n=64, b=256 matrix through the single-matrix FP64 path, and
 bcr), gradient_set (loss and dL/dH over 128 energies through the adjoint,
-forward and backward timed apart) and large_mixed (n=256, b=1024 instances in
-one in-place wave, mixed vs FP64 and the error on a 4-block sub-instance).
+forward and backward timed apart), large_mixed (n=256, b=1024 instances in
+one in-place wave, mixed vs FP64 and the error on a 4-block sub-instance) and
+bcr_batch (256 small matrices through the batched BCR, beside one BCR call
+per matrix and the batched FP64 RGF).
 
 Metric: matrices/s of the whole batch (all ranks).  Under torchrun every rank
 processes its own 512-instance batch (different Hamiltonian seeds): weak
@@ -51,7 +53,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="sinvb", choices=["sinvb", "reference"])
     ap.add_argument("--workload", default="energy_batch",
-                    choices=["energy_batch", "plain_large", "gradient_set", "large_mixed"])
+                    choices=["energy_batch", "plain_large", "gradient_set", "large_mixed", "bcr_batch"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--digits", type=int, default=7, help="int8 slices per value of the mixed products")
     ap.add_argument("--count", type=int, default=0, help="instances (0: the workload's default)")
@@ -641,6 +643,98 @@ def run_plain_large(args, rank, world, local_rank):
     return out
 
 
+def run_bcr_batch(args, rank, world, local_rank):
+    """A batch of small tight-binding matrices (n in [8, 64], b in {32, 64, 128})
+    through the batched BCR: one launch runs phase k of every matrix's
+    reduction / production schedule between the same grid barriers.  Beside it,
+    on the same matrices: one single-matrix BCR call per matrix, and the
+    batched FP64 RGF.  A step is one pass over the batch; every rank inverts
+    its own copy (replicas)."""
+    import torch
+    from sinv_b200 import workloads
+    from sinv_b200.algorithms import BatchPlan, BcrBatchPlan, bcr_batched, bcr_s
+    from oracle import bcr_oracle
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    spec = workloads.bcr_batch_spec(args.count)
+    host = [workloads.tight_binding(n, b, e, seed=s) for (e, n, b, s) in spec]
+    inst = [tuple(torch.from_numpy(x).to(dev) for x in t) for t in host]
+    peak = dmma_peak_tflops(torch)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MB > L2
+    plan = BcrBatchPlan(inst)
+    rgfp = BatchPlan(inst)
+    clocks = Clocks(local_rank) if rank == 0 else None
+    tb, tr, tl = [], [], []
+    for step in range(args.warmup + args.steps):
+        if step == args.warmup and clocks:
+            clocks.start()
+        flush.zero_()
+        mb = _events_ms(torch, lambda: plan.run(stream), stream)
+        flush.zero_()
+        mr = _events_ms(torch, lambda: rgfp.run(stream), stream)
+        if step >= args.warmup:
+            tb.append(_max_over_ranks(torch, world, dev, mb))
+            tr.append(_max_over_ranks(torch, world, dev, mr))
+    clk = clocks.stop() if clocks else None
+    plan.check()
+    rgfp.check()
+    # one single-matrix BCR call per matrix (untimed by the clock sampler; a few steps)
+    for step in range(1 + min(args.steps, 2)):
+        flush.zero_()
+        m = _events_ms(torch, lambda: [bcr_s.bcr_blocks(*t, check=False) for t in inst], stream)
+        if step >= 1:
+            tl.append(_max_over_ranks(torch, world, dev, m))
+    errs = []
+    for k in range(0, len(inst), max(1, len(inst) // 8)):
+        G = plan.results()[k]
+        R = rgfp.results()[k]
+        errs.append(max(float(torch.linalg.norm(g - r) / torch.linalg.norm(r)) for g, r in zip(G, R) if r.numel()))
+    ms = statistics.median(tb)
+    F = sum(workloads.rgf_flops(n, b) for (_, n, b, _) in spec)
+    count = len(spec)
+    del plan, rgfp
+    torch.cuda.empty_cache()
+    # e2e: numpy inputs in, numpy results back, through the public call (schedule build and upload included)
+    te = []
+    bytes_in = sum(x.nbytes for t in host for x in t)
+    for step in range(1 + min(args.steps, 2)):
+        m = _events_ms(torch, lambda: bcr_batched(host, check=False), stream)
+        if step >= 1:
+            te.append(_max_over_ranks(torch, world, dev, m))
+    out = {"metric": "BCR matrices/s, batch of small matrices, FP64", "value": world * count / (ms * 1e-3),
+           "unit": "matrices/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+           "data": "synthetic",
+           "config": {"workload": "bcr_batch(%d matrices, n 8-64, b 32/64/128)" % count, "count": count,
+                      "generator": "tight-binding A(E), energies in [-2, 2], seed 5",
+                      "l2": "256 MB buffer written between timed calls",
+                      "parallelism": "replicas%d" % world},
+           "gpu_launches": args.steps, "rel_err_vs_batched_rgf": max(errs),
+           "roofline": {"bound": "tensor", "achieved": F / (ms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                        "frac": F / (ms * 1e-3) / 1e12 / peak, "traffic": None, "kernel": "bcr_kernel",
+                        "flops": "canonical RGF count 8 b^3 (8(n-1)+n) per matrix (BCR itself does more)",
+                        "peak_source": "sinvb_fp64_mma_peak (DMMA)"},
+           "bcr_per_matrix_calls": {"ms": statistics.median(tl),
+                                    "matrices_per_s": world * count / (statistics.median(tl) * 1e-3)},
+           "rgf_batched_fp64": {"ms": statistics.median(tr),
+                                "matrices_per_s": world * count / (statistics.median(tr) * 1e-3)},
+           "clocks": clk,
+           "e2e": {"value": world * count / (statistics.median(te) * 1e-3), "unit": "matrices/s",
+                   "h2d_bytes_per_step": bytes_in, "d2h_bytes_per_step": bytes_in}}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sample = host[:4]
+        t0 = time.perf_counter()
+        for d, u, l in sample:
+            bcr_oracle.bcr_blocks(d, u, l)
+        t = time.perf_counter() - t0
+        fs = sum(workloads.rgf_flops(n, b) for (_, n, b, _) in spec[:4])
+        v = (fs / t) / (F / count)
+        out["cpu_baseline"] = {"value": v, "unit": "matrices/s", "cores": _blas_threads(), "kind": "port",
+                               "sample": "the first 4 matrices, scaled to the batch's mean size by canonical flops"}
+    return out
+
+
 def plain_cpu(dn, un, ln):
     from oracle import rgf_oracle
     t0 = time.perf_counter()
@@ -864,6 +958,27 @@ def reference_other(args, world):
                                                 "n=256 by the canonical flop count"},
                      "e2e": {"value": v, "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
         return base
+    if args.workload == "bcr_batch":
+        from oracle import bcr_oracle
+        spec = workloads.bcr_batch_spec(args.count)
+        sample = spec[:8]
+        ts = []
+        for _ in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            for (e, n, b, sd) in sample:
+                bcr_oracle.bcr_blocks(*workloads.tight_binding(n, b, e, seed=sd))
+            ts.append(time.perf_counter() - t0)
+        fs = sum(workloads.rgf_flops(n, b) for (_, n, b, _) in sample)
+        F = sum(workloads.rgf_flops(n, b) for (_, n, b, _) in spec)
+        v = (fs / statistics.median(ts)) / (F / len(spec))
+        base.update({"metric": "BCR matrices/s, batch of small matrices, FP64", "value": v, "unit": "matrices/s",
+                     "higher_is_better": True,
+                     "config": {"workload": "bcr_batch(%d matrices, n 8-64, b 32/64/128)" % len(spec)},
+                     "cpu_baseline": {"value": v, "unit": "matrices/s", "cores": _blas_threads(), "kind": "port",
+                                      "sample": "the first 8 matrices per step (reference bcr_serial restated in "
+                                                "numpy), scaled to the batch's mean size by canonical flops"},
+                     "e2e": {"value": v, "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        return base
     base.update({"unavailable": "the reference computes no derivatives (no adjoint of rgf exists in it)"})
     return base
 
@@ -874,7 +989,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if not args.count:
-        args.count = {"energy_batch": 512, "gradient_set": 128, "large_mixed": 13, "plain_large": 1}[args.workload]
+        args.count = {"energy_batch": 512, "gradient_set": 128, "large_mixed": 13, "plain_large": 1,
+                      "bcr_batch": 256}[args.workload]
     if args.impl == "reference":
         if args.workload == "energy_batch":
             run_reference(args, rank, world)
@@ -889,7 +1005,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
         fn = {"energy_batch": run_sinvb, "plain_large": run_plain_large, "gradient_set": run_gradient_set,
-              "large_mixed": run_large_mixed}[args.workload]
+              "large_mixed": run_large_mixed, "bcr_batch": run_bcr_batch}[args.workload]
         out = fn(args, rank, world, local_rank)
         if rank == 0:
             print(json.dumps(out), flush=True)

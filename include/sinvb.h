@@ -242,6 +242,28 @@ int sinvb_rgf_batched_stream_d(const sinvb_batch_desc* descs, int count, unsigne
 int sinvb_rgf_batched_rerun_z(void* workspace, sinvb_stream_t stream);
 int sinvb_rgf_batched_rerun_d(void* workspace, sinvb_stream_t stream);
 
+/* ---- batched BCR: many independent matrices, levels in parallel -------------- */
+/*
+ * bcr_serial (src/sinv/algorithms/bcr/bcr_serial.py:19-62) over a batch of
+ * matrices (descriptors as for the batched RGF; every instance may have its
+ * own n and b).  Phase k of every matrix's reduction / production schedule
+ * runs between the same two grid barriers, so the rows of a level of all
+ * matrices are worked on by every SM at once.  ``status`` (optional, device,
+ * ``count`` ints) gets each matrix's device status; ``flags`` is reserved (0).
+ */
+size_t sinvb_bcr_batched_workspace_size(const sinvb_batch_desc* descs, int count, int dtype, unsigned flags);
+int sinvb_bcr_batched_z(const sinvb_batch_desc* descs, int count, unsigned flags, void* workspace,
+                        size_t workspace_bytes, int* status, sinvb_stream_t stream);
+int sinvb_bcr_batched_d(const sinvb_batch_desc* descs, int count, unsigned flags, void* workspace,
+                        size_t workspace_bytes, int* status, sinvb_stream_t stream);
+/*
+ * Re-runs the batch last uploaded into ``workspace`` by sinvb_bcr_batched_*
+ * with the same ``descs``: two memsets and one launch, no schedule building
+ * and no host-to-device copy (capturable in a CUDA graph).
+ */
+int sinvb_bcr_batched_rerun_z(const sinvb_batch_desc* descs, int count, void* workspace, sinvb_stream_t stream);
+int sinvb_bcr_batched_rerun_d(const sinvb_batch_desc* descs, int count, void* workspace, sinvb_stream_t stream);
+
 /* ---- mixed-precision complex GEMM on the int8 tensor cores ---------------------- */
 /*
  * No reference counterpart (the reference multiplies blocks with numpy/BLAS

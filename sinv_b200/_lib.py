@@ -71,6 +71,11 @@ SIGNATURES = {
     "sinvb_bcr_workspace_size": (_sz, [_i, _i, _i, _u]),
     "sinvb_bcr_z": (_i, _RGF_ARGS),
     "sinvb_bcr_d": (_i, _RGF_ARGS),
+    "sinvb_bcr_batched_workspace_size": (_sz, [_vp, _i, _i, _u]),
+    "sinvb_bcr_batched_z": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp]),
+    "sinvb_bcr_batched_d": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp]),
+    "sinvb_bcr_batched_rerun_z": (_i, [_vp, _i, _vp, _vp]),
+    "sinvb_bcr_batched_rerun_d": (_i, [_vp, _i, _vp, _vp]),
 }
 
 PREC_FP64 = 0

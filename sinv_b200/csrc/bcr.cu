@@ -355,14 +355,29 @@ BcrLayout bcr_layout_and_schedule(int n, int b, const T* diag, const T* upper, c
   return L;
 }
 
+// One matrix (hdr->count == 0): singular blocks are reported in the header's
+// status word.  A batch (hdr->count > 0): op.inst indexes one status word per
+// matrix at hdr->slots_offset, copied to the caller's array at the end.
+// nphases < 0: the phase count stored in the header (a re-run).
 template <class T, int BM, int BN>
 __global__ void __launch_bounds__(kThreads, 1) bcr_kernel(unsigned char* ws, int nphases) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
+  if (nphases < 0) nphases = hdr->sched_phases;
   const ExecOp* ops = reinterpret_cast<const ExecOp*>(ws + hdr->desc_offset);
   const ExecPhase* phases = reinterpret_cast<const ExecPhase*>(ws + hdr->items_offset);
+  const int count = hdr->count;
+  int* op_status = count > 0 ? reinterpret_cast<int*>(ws + hdr->slots_offset) : &hdr->status;
   TeamDyn team{&hdr->barrier_count, &hdr->status, (int)blockIdx.x, (int)gridDim.x, 0u};
-  run_schedule<T, BM, BN>(team, ops, phases, nphases, &hdr->status, reinterpret_cast<T*>(smem_raw));
+  const bool ok = run_schedule<T, BM, BN>(team, ops, phases, nphases, op_status, reinterpret_cast<T*>(smem_raw));
+  if (count > 0 && blockIdx.x == 0) {
+    for (int k = threadIdx.x; k < count; k += blockDim.x) {
+      int st = *((volatile int*)&op_status[k]);
+      if (!ok && st == 0) st = SINVB_STATUS_TIMEOUT;
+      if (hdr->inst_status) hdr->inst_status[k] = st;
+      if (st) report(&hdr->status, st);
+    }
+  }
 }
 
 template <class T, int BM, int BN>
@@ -407,6 +422,146 @@ int run_bcr(const void* diag, const void* upper, const void* lower, int n, int b
   return launch_bcr<T, 32, 32>(ws, (int)s.phases.size(), stream);
 }
 
+// ---------------------------------------------------------------------------
+// A batch of independent matrices in one launch.  Every matrix keeps its own
+// BCR schedule and data region; phase k of the batch is phase k of every
+// matrix that has one, so the rows of a level of all matrices share each grid
+// barrier and small matrices fill the GPU together.  Matrices are independent,
+// so only each matrix's own phase order matters.  Layout: header, one status
+// word per matrix (at a fixed offset, so a re-run can clear them without the
+// schedule), merged op table, merged phases, then the data regions.
+struct BcrBatchLayout {
+  size_t ops_off, phases_off, status_off, total;
+  std::vector<size_t> data_off;
+  int nops, nphases, tile;
+};
+
+int batch_tile(const sinvb_batch_desc* d, int count) {
+  int bmax = 1;
+  for (int k = 0; k < count; k++) bmax = std::max(bmax, d[k].b);
+  return tile_for(bmax);
+}
+
+// Appends phase k of every part to `out`, tagging each op with its matrix.
+void merge_phases(const std::vector<Sched>& parts, Sched& out) {
+  size_t np = 0;
+  for (const Sched& p : parts) np = std::max(np, p.phases.size());
+  for (size_t k = 0; k < np; k++) {
+    out.begin();
+    for (size_t i = 0; i < parts.size(); i++) {
+      if (k >= parts[i].phases.size()) continue;
+      const ExecPhase& ph = parts[i].phases[k];
+      for (int o = ph.op_begin; o < ph.op_end; o++) {
+        ExecOp op = parts[i].ops[o];
+        op.inst = (int)i;
+        out.push(op);
+      }
+    }
+  }
+}
+
+template <class T>
+BcrBatchLayout bcr_batch_layout(const sinvb_batch_desc* d, int count, unsigned char* ws, Sched* out) {
+  BcrBatchLayout L{};
+  L.tile = batch_tile(d, count);
+  std::vector<Sched> parts((size_t)count);
+  std::vector<BcrPlan> plans;
+  plans.reserve((size_t)count);
+  for (int k = 0; k < count; k++) {
+    plans.push_back(bcr_plan(d[k].n, d[k].b));
+    parts[k].bm = parts[k].bn = L.tile;
+    build_bcr<T>(parts[k], plans[k], d[k].n, d[k].b, (const T*)d[k].diag, (const T*)d[k].upper,
+                 (const T*)d[k].lower, (T*)d[k].G_diag, (T*)d[k].G_upper, (T*)d[k].G_lower, (T*)nullptr);
+  }
+  Sched merged;
+  merged.bm = merged.bn = L.tile;
+  merge_phases(parts, merged);
+  L.nops = (int)merged.ops.size();
+  L.nphases = (int)merged.phases.size();
+  L.status_off = sizeof(WsHeader);
+  L.ops_off = align_up(L.status_off + (size_t)count * sizeof(int), 256);
+  L.phases_off = align_up(L.ops_off + (size_t)L.nops * sizeof(ExecOp), 256);
+  size_t off = align_up(L.phases_off + (size_t)L.nphases * sizeof(ExecPhase), 256);
+  L.data_off.resize((size_t)count);
+  for (int k = 0; k < count; k++) {
+    L.data_off[k] = off;
+    off = align_up(off + plans[k].data_elems * sizeof(T), 256);
+  }
+  L.total = off;
+  if (out && ws) {
+    for (int k = 0; k < count; k++) {
+      parts[k] = Sched{};
+      parts[k].bm = parts[k].bn = L.tile;
+      build_bcr<T>(parts[k], plans[k], d[k].n, d[k].b, (const T*)d[k].diag, (const T*)d[k].upper,
+                   (const T*)d[k].lower, (T*)d[k].G_diag, (T*)d[k].G_upper, (T*)d[k].G_lower,
+                   (T*)(ws + L.data_off[k]));
+    }
+    out->bm = out->bn = L.tile;
+    merge_phases(parts, *out);
+  }
+  return L;
+}
+
+template <class T>
+int run_bcr_batched(const sinvb_batch_desc* d, int count, void* workspace, size_t ws_bytes, int* status,
+                    cudaStream_t stream) {
+  if (count < 0 || (count > 0 && !d) || !workspace) return SINVB_EINVAL;
+  if ((uintptr_t)workspace % 256) return SINVB_EWORKSPACE;
+  for (int k = 0; k < count; k++) {
+    const sinvb_batch_desc& e = d[k];
+    if (e.n < 1 || e.b < 1 || !e.diag || !e.G_diag) return SINVB_EINVAL;
+    if (e.n > 1 && (!e.upper || !e.lower || !e.G_upper || !e.G_lower)) return SINVB_EINVAL;
+    for (const void* p : {e.diag, e.upper, e.lower, (const void*)e.G_diag, (const void*)e.G_upper,
+                          (const void*)e.G_lower})
+      if (p && (uintptr_t)p % sizeof(T)) return SINVB_EINVAL;
+  }
+  int rc = check_device();
+  if (rc) return rc;
+  unsigned char* ws = (unsigned char*)workspace;
+  if (count == 0) {
+    if (ws_bytes < sizeof(WsHeader)) return SINVB_EWORKSPACE;
+    SINVB_CUDA(cudaMemsetAsync(ws, 0, sizeof(WsHeader), stream));
+    return SINVB_OK;
+  }
+  Sched s;
+  BcrBatchLayout L = bcr_batch_layout<T>(d, count, ws, &s);
+  if (ws_bytes < L.total) return SINVB_EWORKSPACE;
+  WsHeader h{};
+  h.count = count;
+  h.desc_offset = L.ops_off;
+  h.items_offset = L.phases_off;
+  h.slots_offset = L.status_off;
+  h.inst_status = status;
+  h.sched_phases = L.nphases;
+  SINVB_CUDA(cudaMemcpyAsync(ws, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
+  SINVB_CUDA(cudaMemcpyAsync(ws + L.ops_off, s.ops.data(), s.ops.size() * sizeof(ExecOp), cudaMemcpyHostToDevice,
+                             stream));
+  SINVB_CUDA(cudaMemcpyAsync(ws + L.phases_off, s.phases.data(), s.phases.size() * sizeof(ExecPhase),
+                             cudaMemcpyHostToDevice, stream));
+  SINVB_CUDA(cudaMemsetAsync(ws + L.status_off, 0, (size_t)count * sizeof(int), stream));
+  if (L.tile == 64) return launch_bcr<T, 64, 64>(ws, (int)s.phases.size(), stream);
+  return launch_bcr<T, 32, 32>(ws, (int)s.phases.size(), stream);
+}
+
+// Re-runs the batch uploaded into ws by run_bcr_batched (same descriptors):
+// clears the barrier and status words and launches; the tile comes from the
+// block sizes, the phase count from the header.
+template <class T>
+int rerun_bcr_batched(const sinvb_batch_desc* d, int count, void* workspace, cudaStream_t stream) {
+  if (count < 0 || (count > 0 && !d) || !workspace) return SINVB_EINVAL;
+  if ((uintptr_t)workspace % 256) return SINVB_EWORKSPACE;
+  for (int k = 0; k < count; k++)
+    if (d[k].n < 1 || d[k].b < 1) return SINVB_EINVAL;
+  int rc = check_device();
+  if (rc) return rc;
+  unsigned char* ws = (unsigned char*)workspace;
+  SINVB_CUDA(cudaMemsetAsync(ws, 0, 16, stream));  // status, barrier counter
+  if (count == 0) return SINVB_OK;
+  SINVB_CUDA(cudaMemsetAsync(ws + sizeof(WsHeader), 0, (size_t)count * sizeof(int), stream));
+  if (batch_tile(d, count) == 64) return launch_bcr<T, 64, 64>(ws, -1, stream);
+  return launch_bcr<T, 32, 32>(ws, -1, stream);
+}
+
 }  // namespace
 
 }  // namespace sinvb
@@ -438,6 +593,37 @@ int sinvb_bcr_d(const void* diag, const void* upper, const void* lower, int n, i
                 void* G_upper, void* G_lower, void* workspace, size_t workspace_bytes, sinvb_stream_t stream) {
   return run_bcr<double>(diag, upper, lower, n, b, flags, G_diag, G_upper, G_lower, workspace, workspace_bytes,
                          (cudaStream_t)stream, SINVB_F64);
+}
+
+size_t sinvb_bcr_batched_workspace_size(const sinvb_batch_desc* descs, int count, int dtype, unsigned flags) {
+  (void)flags;
+  if (count < 0 || (count > 0 && !descs)) return 0;
+  if (count == 0) return sizeof(WsHeader);
+  for (int k = 0; k < count; k++)
+    if (descs[k].n < 1 || descs[k].b < 1) return 0;
+  if (dtype == SINVB_C128) return bcr_batch_layout<cplx>(descs, count, nullptr, nullptr).total;
+  if (dtype == SINVB_F64) return bcr_batch_layout<double>(descs, count, nullptr, nullptr).total;
+  return 0;
+}
+
+int sinvb_bcr_batched_z(const sinvb_batch_desc* descs, int count, unsigned flags, void* workspace,
+                        size_t workspace_bytes, int* status, sinvb_stream_t stream) {
+  (void)flags;
+  return run_bcr_batched<cplx>(descs, count, workspace, workspace_bytes, status, (cudaStream_t)stream);
+}
+
+int sinvb_bcr_batched_d(const sinvb_batch_desc* descs, int count, unsigned flags, void* workspace,
+                        size_t workspace_bytes, int* status, sinvb_stream_t stream) {
+  (void)flags;
+  return run_bcr_batched<double>(descs, count, workspace, workspace_bytes, status, (cudaStream_t)stream);
+}
+
+int sinvb_bcr_batched_rerun_z(const sinvb_batch_desc* descs, int count, void* workspace, sinvb_stream_t stream) {
+  return rerun_bcr_batched<cplx>(descs, count, workspace, (cudaStream_t)stream);
+}
+
+int sinvb_bcr_batched_rerun_d(const sinvb_batch_desc* descs, int count, void* workspace, sinvb_stream_t stream) {
+  return rerun_bcr_batched<double>(descs, count, workspace, (cudaStream_t)stream);
 }
 
 }  // extern "C"

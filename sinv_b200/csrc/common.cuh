@@ -85,7 +85,8 @@ struct WsHeader {
   unsigned int* done;         // batched, streamed: done[k] = gen when instance k has finished
   unsigned int gen;
   unsigned int barrier_half[2];  // two-sided RGF: the left and right teams' barrier counters
-  unsigned int pad[28];
+  int sched_phases;              // schedule executor (batched BCR): phases in the uploaded table
+  unsigned int pad[27];
 };
 static_assert(sizeof(WsHeader) == 256, "header is 256 bytes");
 

@@ -22,7 +22,7 @@ struct ExecOp {
   int lda, ldb, ldd, ldc, lda2, ldb2;
   int transpose;
   int unit_start;  // first work unit of the op within its phase
-  int pad;
+  int inst;        // status word of the op (the matrix it belongs to in a batch)
   double alpha;
   const void* A;
   const void* B;
@@ -65,7 +65,7 @@ __device__ void exec_unit(const ExecOp& o, int u, int* status, T* smem) {
     const int tn = (o.N + BN - 1) / BN;
     cta_gemm_tile<T, BM, BN>(g, u / tn, u % tn, smem);
   } else if (o.kind == kExecGj) {
-    cta_gj_invert<T>((T*)o.C, o.ldc, o.M, status, smem);
+    cta_gj_invert<T>((T*)o.C, o.ldc, o.M, status + o.inst, smem);
   } else {
     const T* src = (const T*)o.A;
     T* dst = (T*)o.C;
@@ -84,7 +84,8 @@ __device__ void exec_unit(const ExecOp& o, int u, int* status, T* smem) {
 
 // Runs every phase with the whole team.  Units of a phase are dealt round-robin
 // over the team's CTAs; the op of a unit is found by binary search on
-// unit_start.  Returns false when a barrier gave up.
+// unit_start.  A singular block is reported in status[op.inst].  Returns false
+// when a barrier gave up.
 template <class T, int BM, int BN, class Team>
 __device__ bool run_schedule(Team& team, const ExecOp* ops, const ExecPhase* phases, int nphases, int* status,
                              T* smem) {

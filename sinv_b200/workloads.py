@@ -90,6 +90,13 @@ def gradient_set_spec(count=128, n=32, b=128):
     return [float(e) for e in E], n, b, 3
 
 
+def bcr_batch_spec(count=256):
+    """Per-instance (energy, n, b, hamiltonian seed) of the small-matrix BCR batch:
+    n in [8, 64], b in {32, 64, 128}, the regime where one matrix's BCR levels
+    hold too few block operations to fill the GPU."""
+    return energy_batch_spec(count=count, seed=5, nmin=8, nmax=64, sizes=(32, 64, 128))
+
+
 def large_mixed_spec(count=64, n=256, b=1024):
     """Per-instance (energy, n, b, hamiltonian seed) of the large mixed workload."""
     E = np.random.default_rng(1).uniform(-2.0, 2.0, count)
