@@ -2,7 +2,13 @@
 
 Run from the repository root, with the reference sources available::
 
-    python tests/golden/make_golden.py /path/to/reference
+    python tests/golden/make_golden.py /path/to/reference         # rgf, bcr
+    python tests/golden/make_golden.py /path/to/reference --psr   # psr_outputs.npz
+
+``psr_seqsolve`` (``src/sinv/algorithms/psr/psr_seqsolve.py:20-73``) needs at
+least three MPI processes; it runs here on P threads that exchange its
+``send`` / ``recv`` messages through queues (``ThreadComm``), each thread on
+its own copy of the matrix as each MPI process has.
 
 The reference ``rgf`` (``src/sinv/algorithms/rgf/rgf.py:17-64``) and
 ``bcr_serial`` (``src/sinv/algorithms/bcr/bcr_serial.py:19-62``) are imported
@@ -134,5 +140,92 @@ def main(ref_root):
     print("wrote", path, os.path.getsize(path), "bytes,", len(out), "arrays")
 
 
+# PSR fixtures: the reference test's sizes (tests/psr_tests/psr_test.py:42-52)
+# on 3 and 4 partitions where every partition gets 3 block rows.
+PSR_SIZES = BCR_SIZES
+PSR_VARIANTS = [(True, False), (False, True)]
+
+
+class ThreadComm:
+    """Point-to-point stand-in for ``MPI.COMM_WORLD`` over P threads: ``send`` /
+    ``recv`` by (source, dest, tag) queues, the rank from a thread-local."""
+
+    def __init__(self, size):
+        import queue
+        import threading
+        self.size = size
+        self.local = threading.local()
+        self.q = {(s, d): queue.Queue() for s in range(size) for d in range(size)}
+
+    def Get_rank(self):
+        return self.local.rank
+
+    def Get_size(self):
+        return self.size
+
+    def send(self, obj, dest, tag=0):
+        self.q[(self.local.rank, dest)].put(np.array(obj, copy=True))
+
+    def recv(self, source, tag=0):
+        return self.q[(source, self.local.rank)].get(timeout=600)
+
+
+def run_psr_reference(psr_mod, A, b, P):
+    """The reference ``psr_seqsolve`` (``psr_seqsolve.py:20-73``) on P threads;
+    returns rank 0's G (the aggregated result)."""
+    import threading
+    comm = ThreadComm(P)
+    psr_mod.MPI.COMM_WORLD = comm
+    out, errs = {}, []
+
+    def rank(r):
+        comm.local.rank = r
+        try:
+            out[r] = psr_mod.psr_seqsolve(A.copy(), b)
+        except Exception as e:  # surfaced below
+            errs.append(e)
+
+    ts = [threading.Thread(target=rank, args=(r,)) for r in range(P)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    if errs:
+        raise errs[0]
+    return out[0]
+
+
+def main_psr(ref_root):
+    import_reference(ref_root)  # the same mpi4py / quasi shims as main()
+    from sinv.algorithms.psr import psr_seqsolve as psr_mod
+    out = {}
+    for cplx, sym in PSR_VARIANTS:
+        for N, b in PSR_SIZES:
+            for P in (3, 4):
+                if N // b < 3 * P:
+                    continue
+                A, _ = banded_case(N, b, cplx, sym)
+                G = run_psr_reference(psr_mod, A, b, P)
+                gd, gu, gl = matu.convertDenseToBlkTridiag(G, b)
+                key = f"psr_c{int(cplx)}_s{int(sym)}_N{N}_b{b}_P{P}"
+                out[key + "_in"] = checksum(A)
+                out[key + "_d"], out[key + "_u"], out[key + "_l"] = gd, gu, gl
+    d, u, l = workloads.dominant(24, 16, seed=0)
+    Ad = matu.convertBlkTridiagToDense(d, u, l)
+    out["dom_psr_in"] = checksum(d, u, l)
+    for P in (3, 4, 8):
+        G = run_psr_reference(psr_mod, Ad, 16, P)
+        out[f"dom_psr_P{P}_d"], out[f"dom_psr_P{P}_u"], out[f"dom_psr_P{P}_l"] = \
+            matu.convertDenseToBlkTridiag(G, 16)
+    path = os.path.join(HERE, "psr_outputs.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes,", len(out), "arrays")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    root = args[0] if args else "/root/reference"
+    if "--psr" in sys.argv:
+        main_psr(root)
+    else:
+        main(root)
