@@ -17,8 +17,9 @@ larger than L2 (126 MB) in every wave.
 The default workload is the energy batch in mixed precision (block products
 on the int8 tensor cores for b >= 256, FP64 inverses).  The other workloads:
 plain_large (one n=64, b=256 matrix through the single-matrix FP64 path, and
-bcr), gradient_set (loss and dL/dH over 128 energies through the adjoint,
-forward and backward timed apart), large_mixed (n=256, b=1024 instances in
+bcr, the two-sided RGF and PSR over 3-12 partitions), gradient_set (loss and
+dL/dH over 128 energies through the adjoint, forward and backward timed
+apart), large_mixed (n=256, b=1024 instances in
 one in-place wave, mixed vs FP64 and the error on a 4-block sub-instance) and
 bcr_batch (256 small matrices through the batched BCR, beside one BCR call
 per matrix and the batched FP64 RGF).
@@ -577,11 +578,12 @@ def run_plain_large(args, rank, world, local_rank):
     is one selected inversion; every rank inverts its own copy (replicas)."""
     import torch
     from sinv_b200 import workloads
-    from sinv_b200.algorithms import bcr_s, rgf, rgf2s
+    from sinv_b200.algorithms import bcr_s, psr_s, rgf, rgf2s
     from oracle import rgf_oracle
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     n, b = 64, 256
+    psr_parts = [0, 3, 4, 8, 12]  # 0: the automatic choice
     dn, un, ln = workloads.dominant(n, b, seed=0)
     d, u, l = (torch.from_numpy(x).to(dev) for x in (dn, un, ln))
     peak = dmma_peak_tflops(torch)
@@ -589,6 +591,7 @@ def run_plain_large(args, rank, world, local_rank):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MB > L2
     clocks = Clocks(local_rank) if rank == 0 else None
     ts, tb, t2 = [], [], []
+    tp = {P: [] for P in psr_parts}
     for step in range(args.warmup + args.steps):
         if step == args.warmup and clocks:
             clocks.start()
@@ -598,7 +601,13 @@ def run_plain_large(args, rank, world, local_rank):
         mb = _events_ms(torch, lambda: bcr_s.bcr_blocks(d, u, l, check=False), stream)
         flush.zero_()
         m2 = _events_ms(torch, lambda: rgf2s.rgf2sided(d, u, l, check=False), stream)
+        mp = {}
+        for P in psr_parts:
+            flush.zero_()
+            mp[P] = _events_ms(torch, lambda: psr_s.psr_blocks(d, u, l, partitions=P or None, check=False), stream)
         if step >= args.warmup:
+            for P in psr_parts:
+                tp[P].append(_max_over_ranks(torch, world, dev, mp[P]))
             ts.append(_max_over_ranks(torch, world, dev, ms))
             tb.append(_max_over_ranks(torch, world, dev, mb))
             t2.append(_max_over_ranks(torch, world, dev, m2))
@@ -635,6 +644,11 @@ def run_plain_large(args, rank, world, local_rank):
            "rgf2sided": {"ms": statistics.median(t2), "matrices_per_s": world / (statistics.median(t2) * 1e-3),
                          "rel_err_vs_oracle": max(float(np.linalg.norm(g.cpu().numpy() - r) / np.linalg.norm(r))
                                                   for g, r in zip(rgf2s.rgf2sided(d, u, l), R))},
+           "psr": {"partitions_auto": psr_s.partitions_for(n),
+                   "ms_by_partitions": {str(P or psr_s.partitions_for(n)): statistics.median(tp[P])
+                                        for P in psr_parts},
+                   "rel_err_vs_oracle": max(float(np.linalg.norm(g.cpu().numpy() - r) / np.linalg.norm(r))
+                                            for g, r in zip(psr_s.psr_blocks(d, u, l), R))},
            "clocks": clk,
            "e2e": {"value": world / (statistics.median(te) * 1e-3), "unit": "matrices/s",
                    "h2d_bytes_per_step": bytes_in, "d2h_bytes_per_step": bytes_in}}

@@ -242,6 +242,28 @@ int sinvb_rgf_batched_stream_d(const sinvb_batch_desc* descs, int count, unsigne
 int sinvb_rgf_batched_rerun_z(void* workspace, sinvb_stream_t stream);
 int sinvb_rgf_batched_rerun_d(void* workspace, sinvb_stream_t stream);
 
+/* ---- PSR: parallel Schur reduction over partitions of one matrix -------------- */
+/*
+ * psr_seqsolve (src/sinv/algorithms/psr/psr_seqsolve.py:20-73): the block
+ * rows are split into ``partitions`` parts as psr_utils.py:61-100 does (n / P
+ * rows each, the remainder in the first); every part is reduced by its own
+ * team of CTAs, the 2(P-1) boundary rows form a block tridiagonal reduced
+ * system inverted by the whole grid, and every team then produces its part's
+ * blocks.  The MPI processes of the reference are the teams of one launch.
+ * ``partitions`` = 0 picks about sqrt(n/2); otherwise 3 <= P <= 32 and
+ * n >= 3P (psr_utils.py:55-58), else SINVB_EINVAL.  ``flags`` must be 0; the
+ * whole tridiagonal part of the inverse is written.
+ * sinvb_psr_partitions returns the P a call with these arguments uses, or -1.
+ */
+int sinvb_psr_partitions(int n, int partitions);
+size_t sinvb_psr_workspace_size(int n, int b, int partitions, int dtype, unsigned flags);
+int sinvb_psr_z(const void* diag, const void* upper, const void* lower, int n, int b, int partitions, unsigned flags,
+                void* G_diag, void* G_upper, void* G_lower, void* workspace, size_t workspace_bytes,
+                sinvb_stream_t stream);
+int sinvb_psr_d(const void* diag, const void* upper, const void* lower, int n, int b, int partitions, unsigned flags,
+                void* G_diag, void* G_upper, void* G_lower, void* workspace, size_t workspace_bytes,
+                sinvb_stream_t stream);
+
 /* ---- batched BCR: many independent matrices, levels in parallel -------------- */
 /*
  * bcr_serial (src/sinv/algorithms/bcr/bcr_serial.py:19-62) over a batch of

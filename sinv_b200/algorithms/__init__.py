@@ -2,8 +2,9 @@
 (``src/sinv/algorithms/__init__.py:3-9``): ``rgf`` is the RGF module
 (``rgf.rgf(...)``) and ``bcr_s`` the BCR module (``bcr_s.bcr_serial(...)``).  ``rgf2s`` is the two-sided RGF
 (``rgf2s.rgf2sided(...)``), both halves on one GPU; ``bcr_batched`` runs BCR over
-a batch of matrices in one launch.  The MPI-distributed
-algorithms of the reference (bcr_parallel, psr, pdiv) are not part of this
+a batch of matrices in one launch.  ``psr_s`` is the parallel Schur reduction
+(``psr_s.psr_seqsolve(...)``), its partitions as teams of one launch.  The
+MPI-distributed bcr_parallel and pdiv of the reference are not part of this
 library."""
 
 from . import rgf  # noqa: F401
@@ -11,6 +12,8 @@ from . import rgf2sided as rgf2s  # noqa: F401
 from . import bcr_serial  # noqa: F401
 from . import bcr_serial as bcr_s  # noqa: F401
 from .bcr_serial import BcrBatchPlan, bcr_batched  # noqa: F401
+from . import psr_seqsolve  # noqa: F401
+from . import psr_seqsolve as psr_s  # noqa: F401
 from . import batched  # noqa: F401
 from .batched import BatchPlan, rgf_batched, rgf_batched_host  # noqa: F401
 from . import adjoint  # noqa: F401

@@ -162,41 +162,54 @@ def bcr_batched(instances, check=True, stream=None):
     return plan.results(like=instances[0][0])
 
 
-def bcr_serial(A, blocksize, **kw):
-    """Drop-in for ``bcr_serial(A, blocksize)`` (``bcr_serial.py:19-22``): dense in, dense out."""
-    is_t = dev.is_torch(A)
-    An = A if is_t else np.asarray(A)
-    N = An.shape[0]
-    b = int(blocksize)
-    if An.shape[0] != An.shape[1] or N % b:
-        raise ValueError("A must be square with a size divisible by blocksize")
-    n = N // b
-    if is_t:
-        blocks = An.reshape(n, b, n, b).permute(0, 2, 1, 3)
+def _dense_to_blocks(A, b):
+    """Tridiagonal blocks (diag, upper, lower) of a dense numpy or torch matrix."""
+    n = A.shape[0] // b
+    if dev.is_torch(A):
+        blocks = A.reshape(n, b, n, b).permute(0, 2, 1, 3)
         d = blocks[range(n), range(n)].contiguous()
         u = blocks[range(n - 1), range(1, n)].contiguous() if n > 1 else None
         l = blocks[range(1, n), range(n - 1)].contiguous() if n > 1 else None
-    else:
-        blocks = An.reshape(n, b, n, b).transpose(0, 2, 1, 3)
-        idx = np.arange(n)
-        d = np.ascontiguousarray(blocks[idx, idx])
-        u = np.ascontiguousarray(blocks[idx[:-1], idx[1:]]) if n > 1 else np.zeros((0, b, b), An.dtype)
-        l = np.ascontiguousarray(blocks[idx[1:], idx[:-1]]) if n > 1 else np.zeros((0, b, b), An.dtype)
-    Gd, Gu, Gl = bcr_blocks(d, u, l, **kw)
-    if is_t:
+        return d, u, l
+    An = np.asarray(A)
+    blocks = An.reshape(n, b, n, b).transpose(0, 2, 1, 3)
+    idx = np.arange(n)
+    d = np.ascontiguousarray(blocks[idx, idx])
+    u = np.ascontiguousarray(blocks[idx[:-1], idx[1:]]) if n > 1 else np.zeros((0, b, b), An.dtype)
+    l = np.ascontiguousarray(blocks[idx[1:], idx[:-1]]) if n > 1 else np.zeros((0, b, b), An.dtype)
+    return d, u, l
+
+
+def _blocks_to_dense(G, like):
+    """Dense matrix holding the blocks (G_diag, G_upper, G_lower), zero elsewhere,
+    in the container type of ``like``."""
+    Gd, Gu, Gl = G
+    n, b = Gd.shape[0], Gd.shape[1]
+    N = n * b
+    if dev.is_torch(like):
         torch = dev._torch()
-        G = torch.zeros((N, N), dtype=Gd.dtype, device=Gd.device)
-        Gv = G.view(n, b, n, b).permute(0, 2, 1, 3)
+        out = torch.zeros((N, N), dtype=Gd.dtype, device=Gd.device)
+        Gv = out.view(n, b, n, b).permute(0, 2, 1, 3)
         for i in range(n):
             Gv[i, i] = Gd[i]
             if i < n - 1:
                 Gv[i, i + 1] = Gu[i]
                 Gv[i + 1, i] = Gl[i]
-        return G
-    G = np.zeros((N, N), dtype=Gd.dtype)
+        return out
+    out = np.zeros((N, N), dtype=Gd.dtype)
     for i in range(n):
-        G[i * b:(i + 1) * b, i * b:(i + 1) * b] = Gd[i]
+        out[i * b:(i + 1) * b, i * b:(i + 1) * b] = Gd[i]
         if i < n - 1:
-            G[i * b:(i + 1) * b, (i + 1) * b:(i + 2) * b] = Gu[i]
-            G[(i + 1) * b:(i + 2) * b, i * b:(i + 1) * b] = Gl[i]
-    return G
+            out[i * b:(i + 1) * b, (i + 1) * b:(i + 2) * b] = Gu[i]
+            out[(i + 1) * b:(i + 2) * b, i * b:(i + 1) * b] = Gl[i]
+    return out
+
+
+def bcr_serial(A, blocksize, **kw):
+    """Drop-in for ``bcr_serial(A, blocksize)`` (``bcr_serial.py:19-22``): dense in, dense out."""
+    An = A if dev.is_torch(A) else np.asarray(A)
+    N = An.shape[0]
+    b = int(blocksize)
+    if An.shape[0] != An.shape[1] or N % b:
+        raise ValueError("A must be square with a size divisible by blocksize")
+    return _blocks_to_dense(bcr_blocks(*_dense_to_blocks(An, b), **kw), An)

@@ -1,0 +1,444 @@
+// Parallel Schur reduction (PSR) selected inversion on one GPU.
+//
+// Reference: src/sinv/algorithms/psr/psr_seqsolve.py:20-943 with the
+// partitioning of src/sinv/algorithms/psr/psr_utils.py:61-100.  The reference
+// gives each of P MPI processes one partition of the block rows; here each
+// partition is a team of CTAs of one cooperative launch:
+//
+//   1. every team reduces its partition (psr_seqsolve.py:127-310): the first
+//      partition eliminates downwards, the last upwards, a central partition
+//      downwards from its second row while keeping its top row t, which
+//      gathers the fill-in couplings A[t,i] / A[i,t];
+//   2. the whole grid gathers the reduced system (psr_seqsolve.py:313-467):
+//      the boundary rows [bot_0, t_1, B_1, ..., t_{P-1}], which form a block
+//      tridiagonal system of 2(P-1) blocks, and inverts it with an RGF sweep
+//      (the reference inverts it densely, :470-493; only its tridiagonal
+//      blocks are used afterwards);
+//   3. every team produces its partition's blocks from the boundary blocks of
+//      the inverse (psr_seqsolve.py:647-900).
+//
+// A single matrix then runs chains of about n/P steps per team plus 2(P-1)
+// reduced steps instead of one chain of n.  Inverse blocks are computed once
+// in the reduction and kept (the production's inv(A_ii) is the same inversion
+// of the same block, psr_seqsolve.py:737, :783, :860, :896).
+//
+// Storage (per block row i, b x b blocks in the workspace):
+//   D[i]       reduced diagonal, inverted in place once eliminated
+//   LA[i] UA[i]  first / central partitions: L[i,i-1], U[i-1,i];
+//                last partition: L[i,i+1], U[i+1,i]
+//   LT[j] UT[j]  central partitions: L[t,j], U[j,t]
+//   FR[i] FC[i]  central partitions: fill-in A[t,i], A[i,t] (i >= t+2)
+//   GR[i] GC[i]  central partitions: G[t,i], G[i,t] (i >= t+2)
+#include <algorithm>
+#include <cmath>
+
+#include "block_inverse.cuh"
+#include "host_util.h"
+
+namespace sinvb {
+namespace {
+
+constexpr int kPsrMaxP = 32;
+
+template <class T>
+struct PsrParams {
+  const T* diag;
+  const T* upper;
+  const T* lower;
+  T* Gd;
+  T* Gu;
+  T* Gl;
+  T* D;
+  T* LA;
+  T* UA;
+  T* LT;
+  T* UT;
+  T* FR;
+  T* FC;
+  T* GR;
+  T* GC;
+  T* Rd;   // reduced system: R diagonal, R-1 upper, R-1 lower blocks
+  T* Ru;
+  T* Rl;
+  T* RGd;  // its selected inverse
+  T* RGu;
+  T* RGl;
+  T* T0;   // reduced sweep: T = -G_{i+1} P_{i+1}
+  T* side;  // P + 1 inversion side buffers (one per team, one for the reduced sweep)
+  size_t side_elems;
+  unsigned* team_bar;  // P team barrier counters
+  WsHeader* hdr;
+  int* status;
+  int n, b, P;
+};
+
+// Partition k of n block rows over P (psr_utils.py:61-100): n / P rows each,
+// the remainder in the first.
+__host__ __device__ __forceinline__ int part_start(int n, int P, int k) {
+  const int base = n / P;
+  return k == 0 ? 0 : n - base * (P - k);
+}
+__host__ __device__ __forceinline__ int part_size(int n, int P, int k) {
+  const int base = n / P;
+  return k == 0 ? n - base * (P - 1) : base;
+}
+
+template <class T>
+struct Blk {
+  T* base;
+  size_t bb;
+  __device__ __forceinline__ T* operator()(int i) const { return base + (size_t)i * bb; }
+};
+
+// C = -(A B + A2 B2) (+ D when given)
+template <class T>
+__device__ __forceinline__ GemmOp<T> neg2(int b, const T* A, const T* B, const T* A2, const T* B2, const T* D, T* C) {
+  GemmOp<T> o = make_op<T>(b, b, b, -1.0, A, b, B, b, D, b, C, b);
+  return with_second<T>(o, A2, b, kOpN, B2, b, kOpN, 1);
+}
+
+// Partition reductions, psr_seqsolve.py:160-177 (first), :215-232 (last),
+// :270-310 (central).  D[s .. s+m) starts as a copy of the diagonal.
+template <class T, int BM, int BN, class Team>
+__device__ bool psr_reduce(Team& team, const PsrParams<T>& p, int part, T* side, GemmOp<T>* ops, T* smem) {
+  const int b = p.b, P = p.P, s = part_start(p.n, P, part), m = part_size(p.n, P, part);
+  const size_t bb = (size_t)b * b;
+  const Blk<T> D{p.D, bb}, LA{p.LA, bb}, UA{p.UA, bb}, LT{p.LT, bb}, UT{p.UT, bb}, FR{p.FR, bb}, FC{p.FC, bb};
+  const Blk<const T> up{p.upper, bb}, lo{p.lower, bb};
+  team_copy<T>(team, m * b, b, p.diag + (size_t)s * bb, b, D(s), b);
+  if (!team.sync()) return false;
+  if (part == 0) {
+    for (int i = s + 1; i < s + m; i++) {
+      if (!team_invert<T, BM, BN>(team, D(i - 1), b, b, side, p.status, smem)) return false;
+      ops[0] = make_op<T>(b, b, b, 1.0, lo(i - 1), b, D(i - 1), b, nullptr, 0, LA(i), b);  // L[i,i-1]
+      ops[1] = make_op<T>(b, b, b, 1.0, D(i - 1), b, up(i - 1), b, nullptr, 0, UA(i), b);  // U[i-1,i]
+      team_gemm<T, BM, BN>(team, ops, 2, smem);
+      if (!team.sync()) return false;
+      ops[0] = make_op<T>(b, b, b, -1.0, LA(i), b, up(i - 1), b, D(i), b, D(i), b);
+      team_gemm<T, BM, BN>(team, ops, 1, smem);
+      if (!team.sync()) return false;
+    }
+  } else if (part == P - 1) {
+    for (int i = s + m - 2; i >= s; i--) {
+      if (!team_invert<T, BM, BN>(team, D(i + 1), b, b, side, p.status, smem)) return false;
+      ops[0] = make_op<T>(b, b, b, 1.0, up(i), b, D(i + 1), b, nullptr, 0, LA(i), b);  // L[i,i+1]
+      ops[1] = make_op<T>(b, b, b, 1.0, D(i + 1), b, lo(i), b, nullptr, 0, UA(i), b);  // U[i+1,i]
+      team_gemm<T, BM, BN>(team, ops, 2, smem);
+      if (!team.sync()) return false;
+      ops[0] = make_op<T>(b, b, b, -1.0, LA(i), b, lo(i), b, D(i), b, D(i), b);
+      team_gemm<T, BM, BN>(team, ops, 1, smem);
+      if (!team.sync()) return false;
+    }
+  } else {
+    const int t = s;
+    for (int i = t + 2; i < s + m; i++) {
+      if (!team_invert<T, BM, BN>(team, D(i - 1), b, b, side, p.status, smem)) return false;
+      const T* At = (i - 1 == t + 1) ? lo(t) : FC(i - 1);  // A[i-1,t]
+      const T* Ta = (i - 1 == t + 1) ? up(t) : FR(i - 1);  // A[t,i-1]
+      ops[0] = make_op<T>(b, b, b, 1.0, lo(i - 1), b, D(i - 1), b, nullptr, 0, LA(i), b);  // L[i,i-1]
+      ops[1] = make_op<T>(b, b, b, 1.0, Ta, b, D(i - 1), b, nullptr, 0, LT(i - 1), b);      // L[t,i-1]
+      ops[2] = make_op<T>(b, b, b, 1.0, D(i - 1), b, up(i - 1), b, nullptr, 0, UA(i), b);  // U[i-1,i]
+      ops[3] = make_op<T>(b, b, b, 1.0, D(i - 1), b, At, b, nullptr, 0, UT(i - 1), b);      // U[i-1,t]
+      team_gemm<T, BM, BN>(team, ops, 4, smem);
+      if (!team.sync()) return false;
+      ops[0] = make_op<T>(b, b, b, -1.0, LA(i), b, up(i - 1), b, D(i), b, D(i), b);       // A_ii
+      ops[1] = make_op<T>(b, b, b, -1.0, LT(i - 1), b, At, b, D(t), b, D(t), b);          // A_tt
+      ops[2] = make_op<T>(b, b, b, -1.0, LA(i), b, At, b, nullptr, 0, FC(i), b);          // A[i,t]
+      ops[3] = make_op<T>(b, b, b, -1.0, LT(i - 1), b, up(i - 1), b, nullptr, 0, FR(i), b);  // A[t,i]
+      team_gemm<T, BM, BN>(team, ops, 4, smem);
+      if (!team.sync()) return false;
+    }
+  }
+  return true;
+}
+
+// Partition productions, psr_seqsolve.py:694-737 (first), :740-783 (last),
+// :786-900 (central).  The boundary blocks of G come from the reduced system.
+template <class T, int BM, int BN, class Team>
+__device__ bool psr_produce(Team& team, const PsrParams<T>& p, int part, GemmOp<T>* ops, T* smem) {
+  const int b = p.b, P = p.P, s = part_start(p.n, P, part), m = part_size(p.n, P, part);
+  const size_t bb = (size_t)b * b;
+  const Blk<T> D{p.D, bb}, LA{p.LA, bb}, UA{p.UA, bb}, LT{p.LT, bb}, UT{p.UT, bb}, GR{p.GR, bb}, GC{p.GC, bb};
+  const Blk<T> Gd{p.Gd, bb}, Gu{p.Gu, bb}, Gl{p.Gl, bb};
+  if (part == 0) {
+    for (int i = s + m - 1; i > s; i--) {
+      ops[0] = make_op<T>(b, b, b, -1.0, Gd(i), b, LA(i), b, nullptr, 0, Gl(i - 1), b);  // G[i,i-1]
+      ops[1] = make_op<T>(b, b, b, -1.0, UA(i), b, Gd(i), b, nullptr, 0, Gu(i - 1), b);  // G[i-1,i]
+      team_gemm<T, BM, BN>(team, ops, 2, smem);
+      if (!team.sync()) return false;
+      ops[0] = make_op<T>(b, b, b, -1.0, UA(i), b, Gl(i - 1), b, D(i - 1), b, Gd(i - 1), b);
+      team_gemm<T, BM, BN>(team, ops, 1, smem);
+      if (!team.sync()) return false;
+    }
+  } else if (part == P - 1) {
+    for (int i = s; i < s + m - 1; i++) {
+      ops[0] = make_op<T>(b, b, b, -1.0, Gd(i), b, LA(i), b, nullptr, 0, Gu(i), b);  // G[i,i+1]
+      ops[1] = make_op<T>(b, b, b, -1.0, UA(i), b, Gd(i), b, nullptr, 0, Gl(i), b);  // G[i+1,i]
+      team_gemm<T, BM, BN>(team, ops, 2, smem);
+      if (!team.sync()) return false;
+      ops[0] = make_op<T>(b, b, b, -1.0, UA(i), b, Gu(i), b, D(i + 1), b, Gd(i + 1), b);
+      team_gemm<T, BM, BN>(team, ops, 1, smem);
+      if (!team.sync()) return false;
+    }
+  } else {
+    const int t = s, B = s + m - 1;
+    // G[t,j] / G[j,t] live in GR / GC, except G[t,t+1] / G[t+1,t], which are outputs
+    auto Gtr = [&](int j) { return j == t + 1 ? Gu(t) : GR(j); };
+    auto Gtc = [&](int j) { return j == t + 1 ? Gl(t) : GC(j); };
+    {
+      ops[0] = neg2<T>(b, GC(B), LT(B - 1), Gd(B), LA(B), nullptr, Gl(B - 1));       // G[B,B-1]
+      ops[1] = neg2<T>(b, UA(B), Gd(B), UT(B - 1), GR(B), nullptr, Gu(B - 1));       // G[B-1,B]
+      ops[2] = neg2<T>(b, Gd(t), LT(B - 1), GR(B), LA(B), nullptr, Gtr(B - 1));      // G[t,B-1]
+      ops[3] = neg2<T>(b, UA(B), GC(B), UT(B - 1), Gd(t), nullptr, Gtc(B - 1));      // G[B-1,t]
+      team_gemm<T, BM, BN>(team, ops, 4, smem);
+      if (!team.sync()) return false;
+    }
+    for (int i = B - 1; i >= t + 2; i--) {
+      {  // G_ii = inv(A_ii) - U[i,t] G[t,i] - U[i,i+1] G[i+1,i]
+        ops[0] = neg2<T>(b, UT(i), GR(i), UA(i + 1), Gl(i), D(i), Gd(i));
+        team_gemm<T, BM, BN>(team, ops, 1, smem);
+        if (!team.sync()) return false;
+      }
+      ops[0] = neg2<T>(b, UT(i - 1), GR(i), UA(i), Gd(i), nullptr, Gu(i - 1));     // G[i-1,i]
+      ops[1] = neg2<T>(b, GC(i), LT(i - 1), Gd(i), LA(i), nullptr, Gl(i - 1));     // G[i,i-1]
+      ops[2] = neg2<T>(b, Gd(t), LT(i - 1), GR(i), LA(i), nullptr, Gtr(i - 1));    // G[t,i-1]
+      ops[3] = neg2<T>(b, UA(i), GC(i), UT(i - 1), Gd(t), nullptr, Gtc(i - 1));    // G[i-1,t]
+      team_gemm<T, BM, BN>(team, ops, 4, smem);
+      if (!team.sync()) return false;
+    }
+    ops[0] = neg2<T>(b, UT(t + 1), Gu(t), UA(t + 2), Gl(t + 1), D(t + 1), Gd(t + 1));  // G[t+1,t+1]
+    team_gemm<T, BM, BN>(team, ops, 1, smem);
+    if (!team.sync()) return false;
+  }
+  return true;
+}
+
+// Selected inversion of the reduced system (R blocks in Rd / Ru / Rl) by the
+// whole grid, the recursions of src/sinv/algorithms/rgf/rgf.py:44-62:
+//   forward   X_{i-1} = g_{i-1} U_{i-1} (in RGl),  P_i = L_i g_{i-1} (in RGu),
+//             g_i = (A_ii - P_i U_{i-1})^-1 (in RGd)
+//   backward  T = -G_{i+1} P_{i+1};  G_{i,i+1} = -X_i G_{i+1};  G_ii = g_i - X_i T;
+//             G_{i+1,i} = T
+template <class T, int BM, int BN, class Team>
+__device__ bool reduced_sweep(Team& all, const PsrParams<T>& p, int R, GemmOp<T>* ops, T* smem) {
+  const int b = p.b;
+  const size_t bb = (size_t)b * b;
+  const Blk<T> A{p.Rd, bb}, U{p.Ru, bb}, L{p.Rl, bb}, Gd{p.RGd, bb}, Gu{p.RGu, bb}, Gl{p.RGl, bb};
+  T* Winv = p.side + (size_t)p.P * p.side_elems;
+  team_copy<T>(all, b, b, A(0), b, Gd(0), b);
+  if (!all.sync()) return false;
+  if (!team_invert<T, BM, BN>(all, Gd(0), b, b, Winv, p.status, smem)) return false;
+  for (int i = 1; i < R; i++) {
+    ops[0] = make_op<T>(b, b, b, 1.0, Gd(i - 1), b, U(i - 1), b, nullptr, 0, Gl(i - 1), b);
+    ops[1] = make_op<T>(b, b, b, 1.0, L(i - 1), b, Gd(i - 1), b, nullptr, 0, Gu(i - 1), b);
+    team_gemm<T, BM, BN>(all, ops, 2, smem);
+    if (!all.sync()) return false;
+    ops[0] = make_op<T>(b, b, b, -1.0, Gu(i - 1), b, U(i - 1), b, A(i), b, Gd(i), b);
+    team_gemm<T, BM, BN>(all, ops, 1, smem);
+    if (!all.sync()) return false;
+    if (!team_invert<T, BM, BN>(all, Gd(i), b, b, Winv, p.status, smem)) return false;
+  }
+  for (int i = R - 2; i >= 0; i--) {
+    ops[0] = make_op<T>(b, b, b, -1.0, Gd(i + 1), b, Gu(i), b, nullptr, 0, p.T0, b);
+    team_gemm<T, BM, BN>(all, ops, 1, smem);
+    if (!all.sync()) return false;
+    ops[0] = make_op<T>(b, b, b, -1.0, Gl(i), b, Gd(i + 1), b, nullptr, 0, Gu(i), b);
+    ops[1] = make_op<T>(b, b, b, -1.0, Gl(i), b, p.T0, b, Gd(i), b, Gd(i), b);
+    team_gemm<T, BM, BN>(all, ops, 2, smem);
+    if (!all.sync()) return false;
+    team_copy<T>(all, b, b, p.T0, b, Gl(i), b);
+    if (!all.sync()) return false;
+  }
+  return true;
+}
+
+// Block row of reduced row x: [bot_0, t_1, B_1, ..., t_{P-1}].
+template <class T>
+__device__ __forceinline__ int reduced_row(const PsrParams<T>& p, int x) {
+  if (x == 0) return part_size(p.n, p.P, 0) - 1;
+  const int part = (x + 1) / 2;
+  const int s = part_start(p.n, p.P, part);
+  return (x & 1) ? s : s + part_size(p.n, p.P, part) - 1;
+}
+
+// CTAs are split into P teams (CTA c belongs to team floor(c P / G)); every
+// CTA passes every grid barrier, also after its team gave up on a wait, so the
+// others' waits end.
+template <class T, int BM, int BN>
+__global__ void __launch_bounds__(kThreads, 1) psr_kernel(PsrParams<T> p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* smem = reinterpret_cast<T*>(smem_raw);
+  const int G = gridDim.x, me = blockIdx.x, P = p.P, b = p.b;
+  const size_t bb = (size_t)b * b;
+  const int part = (int)(((long long)me * P) / G);
+  const int first = (int)(((long long)part * G + P - 1) / P);
+  const int last = (int)(((long long)(part + 1) * G + P - 1) / P);
+  TeamDyn all{&p.hdr->barrier_count, p.status, me, G, 0u};
+  TeamDyn team{&p.team_bar[part], p.status, me - first, last - first, 0u};
+  T* side = p.side + (size_t)part * p.side_elems;
+  const int R = 2 * (P - 1);
+
+  GemmOp<T> ops[4];  // one scratch op table for every phase (keeps the stack frame small)
+  psr_reduce<T, BM, BN>(team, p, part, side, ops, smem);
+  if (!all.sync()) return;
+  // gather the reduced system (psr_seqsolve.py:336-384, 410-467)
+  for (int x = 0; x < R; x++) {
+    const int r = reduced_row(p, x);
+    team_copy<T>(all, b, b, p.D + (size_t)r * bb, b, p.Rd + (size_t)x * bb, b);
+    if (x + 1 < R) {
+      const bool link = (x & 1) == 0;  // bot_p -> t_{p+1}: the input couplings; t_p -> B_p: the fill-in
+      const int B = reduced_row(p, x + 1);
+      team_copy<T>(all, b, b, link ? p.upper + (size_t)r * bb : p.FR + (size_t)B * bb, b, p.Ru + (size_t)x * bb, b);
+      team_copy<T>(all, b, b, link ? p.lower + (size_t)r * bb : p.FC + (size_t)B * bb, b, p.Rl + (size_t)x * bb, b);
+    }
+  }
+  if (!all.sync()) return;
+  if (!reduced_sweep<T, BM, BN>(all, p, R, ops, smem)) return;
+  if (!all.sync()) return;
+  // scatter the boundary blocks of the inverse (psr_seqsolve.py:520-645)
+  for (int x = 0; x < R; x++) {
+    const int r = reduced_row(p, x);
+    team_copy<T>(all, b, b, p.RGd + (size_t)x * bb, b, p.Gd + (size_t)r * bb, b);
+    if (x + 1 < R) {
+      const bool link = (x & 1) == 0;
+      const int B = reduced_row(p, x + 1);
+      team_copy<T>(all, b, b, p.RGu + (size_t)x * bb, b, link ? p.Gu + (size_t)r * bb : p.GR + (size_t)B * bb, b);
+      team_copy<T>(all, b, b, p.RGl + (size_t)x * bb, b, link ? p.Gl + (size_t)r * bb : p.GC + (size_t)B * bb, b);
+    }
+  }
+  if (!all.sync()) return;
+  psr_produce<T, BM, BN>(team, p, part, ops, smem);
+}
+
+// Partitions when the caller passes 0: about sqrt(n/2), which balances the
+// 2n/P partition steps against the 4(P-1) steps of the reduced sweep.
+int psr_auto_partitions(int n) {
+  int P = (int)(std::sqrt(n / 2.0) + 0.5);
+  P = std::min(P, std::min(kPsrMaxP, n / 3));
+  return std::max(P, 3);
+}
+
+struct PsrLayout {
+  size_t bar, blocks, reduced, T0, side, total, side_elems;
+};
+
+PsrLayout psr_layout(int n, int b, int P, size_t es) {
+  PsrLayout L{};
+  const size_t bb = (size_t)b * b * es;
+  const int R = 2 * (P - 1);
+  size_t off = sizeof(WsHeader);
+  auto take = [&](size_t bytes) {
+    size_t at = off;
+    off += align_up(bytes, 256);
+    return at;
+  };
+  L.bar = take((size_t)P * sizeof(unsigned));
+  L.blocks = take(9 * (size_t)n * bb);
+  L.reduced = take((size_t)(3 * R - 2) * 2 * bb);
+  L.T0 = take(bb);
+  L.side_elems = invert_side_elems(b);
+  L.side = take((size_t)(P + 1) * L.side_elems * es);
+  L.total = off;
+  return L;
+}
+
+int psr_partitions(int n, int partitions) {
+  const int P = partitions > 0 ? partitions : psr_auto_partitions(n);
+  if (P < 3 || P > kPsrMaxP || n < 3 * P) return -1;  // psr_utils.py:55-58, psr_seqsolve.py:43-44
+  return P;
+}
+
+template <class T>
+int psr_run(const void* diag_, const void* upper_, const void* lower_, int n, int b, int partitions, unsigned flags,
+            void* Gd_, void* Gu_, void* Gl_, void* workspace, size_t workspace_bytes, cudaStream_t stream) {
+  if (n < 1 || b < 1 || !diag_ || !upper_ || !lower_ || !Gd_ || !Gu_ || !Gl_ || !workspace) return SINVB_EINVAL;
+  if (flags) return SINVB_EINVAL;
+  const int P = psr_partitions(n, partitions);
+  if (P < 0) return SINVB_EINVAL;
+  for (const void* q : {diag_, upper_, lower_, (const void*)Gd_, (const void*)Gu_, (const void*)Gl_})
+    if ((uintptr_t)q % sizeof(T)) return SINVB_EINVAL;
+  if ((uintptr_t)workspace % 256) return SINVB_EWORKSPACE;
+  const PsrLayout L = psr_layout(n, b, P, sizeof(T));
+  if (workspace_bytes < L.total) return SINVB_EWORKSPACE;
+  int rc = check_device();
+  if (rc) return rc;
+  unsigned char* ws = (unsigned char*)workspace;
+  const size_t bb = (size_t)b * b;
+  PsrParams<T> p{};
+  p.diag = (const T*)diag_;
+  p.upper = (const T*)upper_;
+  p.lower = (const T*)lower_;
+  p.Gd = (T*)Gd_;
+  p.Gu = (T*)Gu_;
+  p.Gl = (T*)Gl_;
+  T* blk = reinterpret_cast<T*>(ws + L.blocks);
+  T** arrays[9] = {&p.D, &p.LA, &p.UA, &p.LT, &p.UT, &p.FR, &p.FC, &p.GR, &p.GC};
+  for (int k = 0; k < 9; k++) *arrays[k] = blk + (size_t)k * n * bb;
+  const int R = 2 * (P - 1);
+  T* red = reinterpret_cast<T*>(ws + L.reduced);
+  p.Rd = red;
+  p.Ru = p.Rd + (size_t)R * bb;
+  p.Rl = p.Ru + (size_t)(R - 1) * bb;
+  p.RGd = p.Rl + (size_t)(R - 1) * bb;
+  p.RGu = p.RGd + (size_t)R * bb;
+  p.RGl = p.RGu + (size_t)(R - 1) * bb;
+  p.T0 = reinterpret_cast<T*>(ws + L.T0);
+  p.side = reinterpret_cast<T*>(ws + L.side);
+  p.side_elems = L.side_elems;
+  p.team_bar = reinterpret_cast<unsigned*>(ws + L.bar);
+  p.hdr = reinterpret_cast<WsHeader*>(ws);
+  p.status = &p.hdr->status;
+  p.n = n;
+  p.b = b;
+  p.P = P;
+  SINVB_CUDA(cudaMemsetAsync(ws, 0, L.blocks, stream));  // header and team barrier counters
+  void* args[] = {(void*)&p};
+  auto launch = [&](auto kern, size_t smem) -> int {
+    SINVB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    SINVB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
+    if (per_sm < 1) return SINVB_EUNSUPPORTED;
+    const int grid = device_sm_count() * (per_sm > 2 ? 2 : per_sm);
+    if (grid < P) return SINVB_EUNSUPPORTED;
+    SINVB_CUDA(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kThreads), args, smem, stream));
+    return SINVB_OK;
+  };
+  auto smem_for = [](size_t gemm_elems) {
+    const size_t g = gemm_elems * sizeof(T);
+    return g > sizeof(GjShared<T>) ? g : sizeof(GjShared<T>);
+  };
+  if (b <= 32) return launch(psr_kernel<T, 32, 32>, smem_for(gemm_smem_elems<T, 32, 32>()));
+  return launch(psr_kernel<T, 64, 64>, smem_for(gemm_smem_elems<T, 64, 64>()));
+}
+
+}  // namespace
+}  // namespace sinvb
+
+using namespace sinvb;
+
+extern "C" {
+
+int sinvb_psr_partitions(int n, int partitions) { return psr_partitions(n, partitions); }
+
+size_t sinvb_psr_workspace_size(int n, int b, int partitions, int dtype, unsigned flags) {
+  if (flags || b < 1 || (dtype != SINVB_C128 && dtype != SINVB_F64)) return 0;
+  const int P = psr_partitions(n, partitions);
+  if (P < 0) return 0;
+  return psr_layout(n, b, P, dtype == SINVB_C128 ? 16 : 8).total;
+}
+
+int sinvb_psr_z(const void* diag, const void* upper, const void* lower, int n, int b, int partitions, unsigned flags,
+                void* G_diag, void* G_upper, void* G_lower, void* workspace, size_t workspace_bytes,
+                sinvb_stream_t stream) {
+  return psr_run<cplx>(diag, upper, lower, n, b, partitions, flags, G_diag, G_upper, G_lower, workspace,
+                       workspace_bytes, (cudaStream_t)stream);
+}
+
+int sinvb_psr_d(const void* diag, const void* upper, const void* lower, int n, int b, int partitions, unsigned flags,
+                void* G_diag, void* G_upper, void* G_lower, void* workspace, size_t workspace_bytes,
+                sinvb_stream_t stream) {
+  return psr_run<double>(diag, upper, lower, n, b, partitions, flags, G_diag, G_upper, G_lower, workspace,
+                         workspace_bytes, (cudaStream_t)stream);
+}
+
+}  // extern "C"
