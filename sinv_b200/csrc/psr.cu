@@ -18,7 +18,8 @@
 //      the inverse (psr_seqsolve.py:647-900).
 //
 // A single matrix then runs chains of about n/P steps per team plus 2(P-1)
-// reduced steps instead of one chain of n.  Inverse blocks are computed once
+// reduced steps instead of one chain of n.  Every block inverse is refined by
+// one Newton step (refine_invert).  Inverse blocks are computed once
 // in the reduction and kept (the production's inv(A_ii) is the same inversion
 // of the same block, psr_seqsolve.py:737, :783, :860, :896).
 //
@@ -66,6 +67,7 @@ struct PsrParams {
   T* T0;   // reduced sweep: T = -G_{i+1} P_{i+1}
   T* side;  // P + 1 inversion side buffers (one per team, one for the reduced sweep)
   size_t side_elems;
+  T* work;  // P + 1 pairs of b x b blocks for the refined inversions
   unsigned* team_bar;  // P team barrier counters
   WsHeader* hdr;
   int* status;
@@ -97,10 +99,33 @@ __device__ __forceinline__ GemmOp<T> neg2(int b, const T* A, const T* B, const T
   return with_second<T>(o, A2, b, kOpN, B2, b, kOpN, 1);
 }
 
+// In-place inverse of the b x b block a, refined by one Newton step
+// X1 = X0 + X0 (I - A X0) = 2 X0 - X0 (A X0).  The reference inverts with
+// LAPACK (partial pivoting); team_invert is a pivot-free blocked Gauss-Jordan,
+// whose error grows on the undamped indefinite blocks PSR inverts (a central
+// partition's first eliminated block is E - H_ii as given), and the step
+// squares its residual.  work: two b x b blocks.
+template <class T, int BM, int BN, class Team>
+__device__ bool refine_invert(Team& team, T* a, int b, T* work, T* side, int* status, GemmOp<T>* ops, T* smem) {
+  T* X = work;
+  T* AX = work + (size_t)b * b;
+  team_copy<T>(team, b, b, a, b, X, b);
+  if (!team.sync()) return false;
+  if (!team_invert<T, BM, BN>(team, X, b, b, side, status, smem)) return false;
+  ops[0] = make_op<T>(b, b, b, 1.0, a, b, X, b, nullptr, 0, AX, b);  // A X0
+  team_gemm<T, BM, BN>(team, ops, 1, smem);
+  if (!team.sync()) return false;
+  ops[0] = make_op<T>(b, b, b, -1.0, X, b, AX, b, X, b, a, b);       // 2 X0 - X0 (A X0)
+  ops[0].beta = 2.0;
+  team_gemm<T, BM, BN>(team, ops, 1, smem);
+  return team.sync();
+}
+
 // Partition reductions, psr_seqsolve.py:160-177 (first), :215-232 (last),
 // :270-310 (central).  D[s .. s+m) starts as a copy of the diagonal.
 template <class T, int BM, int BN, class Team>
-__device__ bool psr_reduce(Team& team, const PsrParams<T>& p, int part, T* side, GemmOp<T>* ops, T* smem) {
+__device__ bool psr_reduce(Team& team, const PsrParams<T>& p, int part, T* side, T* work, GemmOp<T>* ops,
+                           T* smem) {
   const int b = p.b, P = p.P, s = part_start(p.n, P, part), m = part_size(p.n, P, part);
   const size_t bb = (size_t)b * b;
   const Blk<T> D{p.D, bb}, LA{p.LA, bb}, UA{p.UA, bb}, LT{p.LT, bb}, UT{p.UT, bb}, FR{p.FR, bb}, FC{p.FC, bb};
@@ -109,7 +134,7 @@ __device__ bool psr_reduce(Team& team, const PsrParams<T>& p, int part, T* side,
   if (!team.sync()) return false;
   if (part == 0) {
     for (int i = s + 1; i < s + m; i++) {
-      if (!team_invert<T, BM, BN>(team, D(i - 1), b, b, side, p.status, smem)) return false;
+      if (!refine_invert<T, BM, BN>(team, D(i - 1), b, work, side, p.status, ops, smem)) return false;
       ops[0] = make_op<T>(b, b, b, 1.0, lo(i - 1), b, D(i - 1), b, nullptr, 0, LA(i), b);  // L[i,i-1]
       ops[1] = make_op<T>(b, b, b, 1.0, D(i - 1), b, up(i - 1), b, nullptr, 0, UA(i), b);  // U[i-1,i]
       team_gemm<T, BM, BN>(team, ops, 2, smem);
@@ -120,7 +145,7 @@ __device__ bool psr_reduce(Team& team, const PsrParams<T>& p, int part, T* side,
     }
   } else if (part == P - 1) {
     for (int i = s + m - 2; i >= s; i--) {
-      if (!team_invert<T, BM, BN>(team, D(i + 1), b, b, side, p.status, smem)) return false;
+      if (!refine_invert<T, BM, BN>(team, D(i + 1), b, work, side, p.status, ops, smem)) return false;
       ops[0] = make_op<T>(b, b, b, 1.0, up(i), b, D(i + 1), b, nullptr, 0, LA(i), b);  // L[i,i+1]
       ops[1] = make_op<T>(b, b, b, 1.0, D(i + 1), b, lo(i), b, nullptr, 0, UA(i), b);  // U[i+1,i]
       team_gemm<T, BM, BN>(team, ops, 2, smem);
@@ -132,7 +157,7 @@ __device__ bool psr_reduce(Team& team, const PsrParams<T>& p, int part, T* side,
   } else {
     const int t = s;
     for (int i = t + 2; i < s + m; i++) {
-      if (!team_invert<T, BM, BN>(team, D(i - 1), b, b, side, p.status, smem)) return false;
+      if (!refine_invert<T, BM, BN>(team, D(i - 1), b, work, side, p.status, ops, smem)) return false;
       const T* At = (i - 1 == t + 1) ? lo(t) : FC(i - 1);  // A[i-1,t]
       const T* Ta = (i - 1 == t + 1) ? up(t) : FR(i - 1);  // A[t,i-1]
       ops[0] = make_op<T>(b, b, b, 1.0, lo(i - 1), b, D(i - 1), b, nullptr, 0, LA(i), b);  // L[i,i-1]
@@ -225,9 +250,10 @@ __device__ bool reduced_sweep(Team& all, const PsrParams<T>& p, int R, GemmOp<T>
   const size_t bb = (size_t)b * b;
   const Blk<T> A{p.Rd, bb}, U{p.Ru, bb}, L{p.Rl, bb}, Gd{p.RGd, bb}, Gu{p.RGu, bb}, Gl{p.RGl, bb};
   T* Winv = p.side + (size_t)p.P * p.side_elems;
+  T* work = p.work + (size_t)p.P * 2 * bb;
   team_copy<T>(all, b, b, A(0), b, Gd(0), b);
   if (!all.sync()) return false;
-  if (!team_invert<T, BM, BN>(all, Gd(0), b, b, Winv, p.status, smem)) return false;
+  if (!refine_invert<T, BM, BN>(all, Gd(0), b, work, Winv, p.status, ops, smem)) return false;
   for (int i = 1; i < R; i++) {
     ops[0] = make_op<T>(b, b, b, 1.0, Gd(i - 1), b, U(i - 1), b, nullptr, 0, Gl(i - 1), b);
     ops[1] = make_op<T>(b, b, b, 1.0, L(i - 1), b, Gd(i - 1), b, nullptr, 0, Gu(i - 1), b);
@@ -236,7 +262,7 @@ __device__ bool reduced_sweep(Team& all, const PsrParams<T>& p, int R, GemmOp<T>
     ops[0] = make_op<T>(b, b, b, -1.0, Gu(i - 1), b, U(i - 1), b, A(i), b, Gd(i), b);
     team_gemm<T, BM, BN>(all, ops, 1, smem);
     if (!all.sync()) return false;
-    if (!team_invert<T, BM, BN>(all, Gd(i), b, b, Winv, p.status, smem)) return false;
+    if (!refine_invert<T, BM, BN>(all, Gd(i), b, work, Winv, p.status, ops, smem)) return false;
   }
   for (int i = R - 2; i >= 0; i--) {
     ops[0] = make_op<T>(b, b, b, -1.0, Gd(i + 1), b, Gu(i), b, nullptr, 0, p.T0, b);
@@ -279,7 +305,7 @@ __global__ void __launch_bounds__(kThreads, 1) psr_kernel(PsrParams<T> p) {
   const int R = 2 * (P - 1);
 
   GemmOp<T> ops[4];  // one scratch op table for every phase (keeps the stack frame small)
-  psr_reduce<T, BM, BN>(team, p, part, side, ops, smem);
+  psr_reduce<T, BM, BN>(team, p, part, side, p.work + (size_t)part * 2 * bb, ops, smem);
   if (!all.sync()) return;
   // gather the reduced system (psr_seqsolve.py:336-384, 410-467)
   for (int x = 0; x < R; x++) {
@@ -319,7 +345,7 @@ int psr_auto_partitions(int n) {
 }
 
 struct PsrLayout {
-  size_t bar, blocks, reduced, T0, side, total, side_elems;
+  size_t bar, blocks, reduced, T0, work, side, total, side_elems;
 };
 
 PsrLayout psr_layout(int n, int b, int P, size_t es) {
@@ -336,6 +362,7 @@ PsrLayout psr_layout(int n, int b, int P, size_t es) {
   L.blocks = take(9 * (size_t)n * bb);
   L.reduced = take((size_t)(3 * R - 2) * 2 * bb);
   L.T0 = take(bb);
+  L.work = take((size_t)(P + 1) * 2 * bb);
   L.side_elems = invert_side_elems(b);
   L.side = take((size_t)(P + 1) * L.side_elems * es);
   L.total = off;
@@ -384,6 +411,7 @@ int psr_run(const void* diag_, const void* upper_, const void* lower_, int n, in
   p.RGl = p.RGu + (size_t)(R - 1) * bb;
   p.T0 = reinterpret_cast<T*>(ws + L.T0);
   p.side = reinterpret_cast<T*>(ws + L.side);
+  p.work = reinterpret_cast<T*>(ws + L.work);
   p.side_elems = L.side_elems;
   p.team_bar = reinterpret_cast<unsigned*>(ws + L.bar);
   p.hdr = reinterpret_cast<WsHeader*>(ws);
