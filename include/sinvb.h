@@ -263,6 +263,25 @@ int sinvb_psr_z(const void* diag, const void* upper, const void* lower, int n, i
 int sinvb_psr_d(const void* diag, const void* upper, const void* lower, int n, int b, int partitions, unsigned flags,
                 void* G_diag, void* G_upper, void* G_lower, void* workspace, size_t workspace_bytes,
                 sinvb_stream_t stream);
+/*
+ * One partition of a multi-GPU PSR on this GPU: what reference process
+ * ``part`` of ``partitions`` does (psr_seqsolve.py:52-70), every process
+ * holding the whole block arrays.  stage 0 reduces the partition and writes
+ * its part of the reduced system to ``boundary`` (4 b x b blocks, device):
+ * first partition D[B]; last D[t]; central D[t], D[B], A[t,B], A[B,t] (t, B
+ * the partition's first and last block rows).  stage 1 takes the boundary
+ * blocks of the reduced system's inverse in the same slots (G[B,B]; G[t,t];
+ * G[t,t], G[B,B], G[t,B], G[B,t]) and writes the partition's rows of G_diag /
+ * G_upper / G_lower (the coupling to the next partition, G[B,B+1] and
+ * G[B+1,B], comes from the reduced inverse and is the caller's to store).
+ * Use the same workspace (sinvb_psr_workspace_size) for both stages.
+ */
+int sinvb_psr_part_z(const void* diag, const void* upper, const void* lower, int n, int b, int partitions, int part,
+                     int stage, void* boundary, void* G_diag, void* G_upper, void* G_lower, void* workspace,
+                     size_t workspace_bytes, sinvb_stream_t stream);
+int sinvb_psr_part_d(const void* diag, const void* upper, const void* lower, int n, int b, int partitions, int part,
+                     int stage, void* boundary, void* G_diag, void* G_upper, void* G_lower, void* workspace,
+                     size_t workspace_bytes, sinvb_stream_t stream);
 
 /* ---- batched BCR: many independent matrices, levels in parallel -------------- */
 /*

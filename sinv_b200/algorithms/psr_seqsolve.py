@@ -82,3 +82,125 @@ def psr_seqsolve(A, blocksize, partitions=None, **kw):
         raise ValueError("A must be square with a size divisible by blocksize")
     G = psr_blocks(*_dense_to_blocks(An, b), partitions=partitions, **kw)
     return _blocks_to_dense(G, An)
+
+
+# --------------------------------------------------------------------------- one partition per GPU
+def part_rows(n, P, part):
+    """(first row t, last row B) of partition ``part`` (``psr_utils.py:61-100``)."""
+    base = n // P
+    s = 0 if part == 0 else n - base * (P - part)
+    m = n - base * (P - 1) if part == 0 else base
+    return s, s + m - 1
+
+
+def reduced_rows(n, P):
+    """Block rows of the reduced system: [B_0, t_1, B_1, ..., t_{P-1}]
+    (``psr_seqsolve.py:336-384``)."""
+    rows = [part_rows(n, P, 0)[1]]
+    for p in range(1, P - 1):
+        rows += list(part_rows(n, P, p))
+    rows.append(part_rows(n, P, P - 1)[0])
+    return rows
+
+
+def reduced_system(boundaries, A_upper, A_lower, n, P):
+    """The block tridiagonal reduced system from every partition's boundary
+    slots (in partition order) and the input couplings between partitions.
+    Returns ``(R_diag, R_upper, R_lower)`` stacked like ``boundaries[0]``
+    (host bookkeeping on tensors of any device)."""
+    import torch
+    rows = reduced_rows(n, P)
+    diag = [boundaries[0][0]]
+    for p in range(1, P - 1):
+        diag += [boundaries[p][0], boundaries[p][1]]
+    diag.append(boundaries[P - 1][0])
+    upper, lower = [], []
+    for x in range(len(rows) - 1):
+        if x % 2 == 0:  # B_p -> t_{p+1}: the input coupling
+            upper.append(A_upper[rows[x]])
+            lower.append(A_lower[rows[x]])
+        else:           # t_p -> B_p of a central partition: its fill-in
+            p = (x + 1) // 2
+            upper.append(boundaries[p][2])
+            lower.append(boundaries[p][3])
+    return torch.stack(diag), torch.stack(upper), torch.stack(lower)
+
+
+def boundary_inverse(RG, part, P):
+    """The four boundary slots partition ``part`` needs from the reduced
+    system's inverse ``RG = (G_diag, G_upper, G_lower)``, and its coupling to
+    the next partition ``(G[B,B+1], G[B+1,B])`` (None for the last)."""
+    import torch
+    Rd, Ru, Rl = RG
+    zero = torch.zeros_like(Rd[0])
+    if part == 0:
+        slots = [Rd[0], zero, zero, zero]
+    elif part == P - 1:
+        slots = [Rd[-1], zero, zero, zero]
+    else:
+        x = 2 * part - 1
+        slots = [Rd[x], Rd[x + 1], Ru[x], Rl[x]]
+    link = (Ru[2 * part], Rl[2 * part]) if part < P - 1 else None
+    return torch.stack(slots), link
+
+
+class PsrPart:
+    """Partition ``part`` of a ``partitions``-way PSR on this GPU
+    (``sinvb_psr_part_*``): ``reduce()`` returns the boundary slots,
+    ``produce(slots, link)`` fills the partition's rows of G.  The block arrays
+    are the whole matrix, as every reference process holds it."""
+
+    def __init__(self, A_diag, A_upper, A_lower, partitions, part, device=None):
+        torch = dev._torch()
+        self.lib = _lib.load()
+        self.in_dt = dev.torch_dtype(A_diag)
+        self.wide = {torch.complex64: torch.complex128, torch.float32: torch.float64}.get(self.in_dt, self.in_dt)
+        self.code = _lib.dtype_code(self.wide)
+        if self.code not in (_lib.C128, _lib.F64):
+            raise TypeError("unsupported dtype %s" % self.in_dt)
+        with torch.cuda.device(device if device is not None else torch.cuda.current_device()):
+            self.d = dev.to_device(A_diag, self.wide)
+            self.u = dev.to_device(A_upper, self.wide)
+            self.l = dev.to_device(A_lower, self.wide)
+        self.n, self.b = int(self.d.shape[0]), int(self.d.shape[1])
+        self.P = partitions_for(self.n, partitions)
+        if self.P < 0 or not 0 <= part < self.P:
+            raise ValueError("PSR needs 3 <= partitions <= 32, 3 block rows per partition and 0 <= part < "
+                             "partitions (n=%d, partitions=%s, part=%d)" % (self.n, partitions, part))
+        self.part = part
+        self.device = self.d.device
+        n, b = self.n, self.b
+        self.G = tuple(torch.zeros((m, b, b), dtype=self.wide, device=self.device) for m in (n, n - 1, n - 1))
+        self.slots = torch.zeros((4, b, b), dtype=self.wide, device=self.device)
+        with torch.cuda.device(self.device):
+            self.ws = dev.workspace(self.lib.sinvb_psr_workspace_size(n, b, self.P, self.code, 0), self.device)
+        self.rows = part_rows(n, self.P, part)
+
+    def _stage(self, stage, stream=None):
+        torch = dev._torch()
+        fn = self.lib.sinvb_psr_part_z if self.code == _lib.C128 else self.lib.sinvb_psr_part_d
+        with torch.cuda.device(self.device):
+            rc = fn(dev.ptr(self.d), dev.ptr(self.u), dev.ptr(self.l), self.n, self.b, self.P, self.part, stage,
+                    dev.ptr(self.slots), dev.ptr(self.G[0]), dev.ptr(self.G[1]), dev.ptr(self.G[2]),
+                    dev.ptr(self.ws), self.ws.numel(), dev.stream_handle(stream))
+            _lib.check(rc, "sinvb_psr_part")
+
+    def reduce(self, stream=None):
+        self._stage(0, stream)
+        return self.slots
+
+    def produce(self, slots, link=None, stream=None, check=True):
+        self.slots.copy_(slots)
+        self._stage(1, stream)
+        B = self.rows[1]
+        if link is not None:
+            self.G[1][B].copy_(link[0])
+            self.G[2][B].copy_(link[1])
+        if check:
+            dev.raise_for_status(dev.read_status(self.lib, self.ws, stream), "psr part %d" % self.part)
+        return self.G
+
+    def solve_reduced(self, Rd, Ru, Rl):
+        """Selected inverse of the reduced system (every rank solves it)."""
+        from .rgf import rgf_blocks
+        return rgf_blocks(Rd, Ru, Rl)

@@ -376,28 +376,29 @@ int psr_partitions(int n, int partitions) {
 }
 
 template <class T>
-int psr_run(const void* diag_, const void* upper_, const void* lower_, int n, int b, int partitions, unsigned flags,
-            void* Gd_, void* Gu_, void* Gl_, void* workspace, size_t workspace_bytes, cudaStream_t stream) {
-  if (n < 1 || b < 1 || !diag_ || !upper_ || !lower_ || !Gd_ || !Gu_ || !Gl_ || !workspace) return SINVB_EINVAL;
-  if (flags) return SINVB_EINVAL;
-  const int P = psr_partitions(n, partitions);
+int psr_check(const void* diag, const void* upper, const void* lower, int n, int b, int P, const void* Gd,
+              const void* Gu, const void* Gl, const void* workspace, size_t workspace_bytes) {
+  if (n < 1 || b < 1 || !diag || !upper || !lower || !Gd || !Gu || !Gl || !workspace) return SINVB_EINVAL;
   if (P < 0) return SINVB_EINVAL;
-  for (const void* q : {diag_, upper_, lower_, (const void*)Gd_, (const void*)Gu_, (const void*)Gl_})
+  for (const void* q : {diag, upper, lower, Gd, Gu, Gl})
     if ((uintptr_t)q % sizeof(T)) return SINVB_EINVAL;
   if ((uintptr_t)workspace % 256) return SINVB_EWORKSPACE;
+  if (workspace_bytes < psr_layout(n, b, P, sizeof(T)).total) return SINVB_EWORKSPACE;
+  return check_device();
+}
+
+template <class T>
+PsrParams<T> psr_params(const void* diag, const void* upper, const void* lower, int n, int b, int P, void* Gd,
+                        void* Gu, void* Gl, unsigned char* ws) {
   const PsrLayout L = psr_layout(n, b, P, sizeof(T));
-  if (workspace_bytes < L.total) return SINVB_EWORKSPACE;
-  int rc = check_device();
-  if (rc) return rc;
-  unsigned char* ws = (unsigned char*)workspace;
   const size_t bb = (size_t)b * b;
   PsrParams<T> p{};
-  p.diag = (const T*)diag_;
-  p.upper = (const T*)upper_;
-  p.lower = (const T*)lower_;
-  p.Gd = (T*)Gd_;
-  p.Gu = (T*)Gu_;
-  p.Gl = (T*)Gl_;
+  p.diag = (const T*)diag;
+  p.upper = (const T*)upper;
+  p.lower = (const T*)lower;
+  p.Gd = (T*)Gd;
+  p.Gu = (T*)Gu;
+  p.Gl = (T*)Gl;
   T* blk = reinterpret_cast<T*>(ws + L.blocks);
   T** arrays[9] = {&p.D, &p.LA, &p.UA, &p.LT, &p.UT, &p.FR, &p.FC, &p.GR, &p.GC};
   for (int k = 0; k < 9; k++) *arrays[k] = blk + (size_t)k * n * bb;
@@ -419,24 +420,103 @@ int psr_run(const void* diag_, const void* upper_, const void* lower_, int n, in
   p.n = n;
   p.b = b;
   p.P = P;
-  SINVB_CUDA(cudaMemsetAsync(ws, 0, L.blocks, stream));  // header and team barrier counters
+  return p;
+}
+
+// Cooperative launch on the whole GPU (up to two CTAs per SM).
+template <class T, class Kern>
+int psr_launch(Kern kern, void** args, int min_grid, cudaStream_t stream) {
+  const size_t g = (size_t)gemm_smem_elems<T, 64, 64>() * sizeof(T);
+  const size_t smem = g > sizeof(GjShared<T>) ? g : sizeof(GjShared<T>);
+  SINVB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  SINVB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
+  if (per_sm < 1) return SINVB_EUNSUPPORTED;
+  const int grid = device_sm_count() * (per_sm > 2 ? 2 : per_sm);
+  if (grid < min_grid) return SINVB_EUNSUPPORTED;
+  SINVB_CUDA(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kThreads), args, smem, stream));
+  return SINVB_OK;
+}
+
+template <class T>
+int psr_run(const void* diag, const void* upper, const void* lower, int n, int b, int partitions, unsigned flags,
+            void* Gd, void* Gu, void* Gl, void* workspace, size_t workspace_bytes, cudaStream_t stream) {
+  if (flags) return SINVB_EINVAL;
+  const int P = psr_partitions(n, partitions);
+  int rc = psr_check<T>(diag, upper, lower, n, b, P, Gd, Gu, Gl, workspace, workspace_bytes);
+  if (rc) return rc;
+  unsigned char* ws = (unsigned char*)workspace;
+  PsrParams<T> p = psr_params<T>(diag, upper, lower, n, b, P, Gd, Gu, Gl, ws);
+  SINVB_CUDA(cudaMemsetAsync(ws, 0, psr_layout(n, b, P, sizeof(T)).blocks, stream));  // header, team barriers
   void* args[] = {(void*)&p};
-  auto launch = [&](auto kern, size_t smem) -> int {
-    SINVB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    SINVB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
-    if (per_sm < 1) return SINVB_EUNSUPPORTED;
-    const int grid = device_sm_count() * (per_sm > 2 ? 2 : per_sm);
-    if (grid < P) return SINVB_EUNSUPPORTED;
-    SINVB_CUDA(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kThreads), args, smem, stream));
-    return SINVB_OK;
-  };
-  auto smem_for = [](size_t gemm_elems) {
-    const size_t g = gemm_elems * sizeof(T);
-    return g > sizeof(GjShared<T>) ? g : sizeof(GjShared<T>);
-  };
-  if (b <= 32) return launch(psr_kernel<T, 32, 32>, smem_for(gemm_smem_elems<T, 32, 32>()));
-  return launch(psr_kernel<T, 64, 64>, smem_for(gemm_smem_elems<T, 64, 64>()));
+  if (b <= 32) return psr_launch<T>(psr_kernel<T, 32, 32>, args, P, stream);
+  return psr_launch<T>(psr_kernel<T, 64, 64>, args, P, stream);
+}
+
+// One partition on its own GPU, the form a rank of a multi-GPU PSR runs
+// (psr_seqsolve.py:52-70 on process `part`), with the whole grid as the team.
+// stage 0 reduces the partition and writes its part of the reduced system to
+// four boundary slots (psr_seqsolve.py:387-467): first partition D[B]; last
+// D[t]; central D[t], D[B], A[t,B], A[B,t].  stage 1 reads the boundary
+// blocks of the inverse from the same slots (first G[B,B]; last G[t,t];
+// central G[t,t], G[B,B], G[t,B], G[B,t]; psr_seqsolve.py:564-644) and
+// produces the partition.  The workspace carries the reduction from stage 0
+// to stage 1.
+template <class T, int BM, int BN>
+__global__ void __launch_bounds__(kThreads, 1) psr_part_kernel(PsrParams<T> p, int part, int stage, T* bnd) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* smem = reinterpret_cast<T*>(smem_raw);
+  const int P = p.P, b = p.b;
+  const size_t bb = (size_t)b * b;
+  const int t = part_start(p.n, P, part), B = t + part_size(p.n, P, part) - 1;
+  TeamDyn all{&p.hdr->barrier_count, p.status, (int)blockIdx.x, (int)gridDim.x, 0u};
+  GemmOp<T> ops[4];
+  T* slot[4] = {bnd, bnd + bb, bnd + 2 * bb, bnd + 3 * bb};
+  if (stage == 0) {
+    if (!psr_reduce<T, BM, BN>(all, p, part, p.side, p.work, ops, smem)) return;
+    if (part == 0) {
+      team_copy<T>(all, b, b, p.D + (size_t)B * bb, b, slot[0], b);
+    } else if (part == P - 1) {
+      team_copy<T>(all, b, b, p.D + (size_t)t * bb, b, slot[0], b);
+    } else {
+      team_copy<T>(all, b, b, p.D + (size_t)t * bb, b, slot[0], b);
+      team_copy<T>(all, b, b, p.D + (size_t)B * bb, b, slot[1], b);
+      team_copy<T>(all, b, b, p.FR + (size_t)B * bb, b, slot[2], b);
+      team_copy<T>(all, b, b, p.FC + (size_t)B * bb, b, slot[3], b);
+    }
+    all.sync();
+  } else {
+    if (part == 0) {
+      team_copy<T>(all, b, b, slot[0], b, p.Gd + (size_t)B * bb, b);
+    } else if (part == P - 1) {
+      team_copy<T>(all, b, b, slot[0], b, p.Gd + (size_t)t * bb, b);
+    } else {
+      team_copy<T>(all, b, b, slot[0], b, p.Gd + (size_t)t * bb, b);
+      team_copy<T>(all, b, b, slot[1], b, p.Gd + (size_t)B * bb, b);
+      team_copy<T>(all, b, b, slot[2], b, p.GR + (size_t)B * bb, b);
+      team_copy<T>(all, b, b, slot[3], b, p.GC + (size_t)B * bb, b);
+    }
+    if (!all.sync()) return;
+    psr_produce<T, BM, BN>(all, p, part, ops, smem);
+  }
+}
+
+template <class T>
+int psr_part_run(const void* diag, const void* upper, const void* lower, int n, int b, int partitions, int part,
+                 int stage, void* boundary, void* Gd, void* Gu, void* Gl, void* workspace, size_t workspace_bytes,
+                 cudaStream_t stream) {
+  const int P = psr_partitions(n, partitions);
+  if (P < 0 || part < 0 || part >= P || (stage != 0 && stage != 1) || !boundary) return SINVB_EINVAL;
+  if ((uintptr_t)boundary % sizeof(T)) return SINVB_EINVAL;
+  int rc = psr_check<T>(diag, upper, lower, n, b, P, Gd, Gu, Gl, workspace, workspace_bytes);
+  if (rc) return rc;
+  unsigned char* ws = (unsigned char*)workspace;
+  PsrParams<T> p = psr_params<T>(diag, upper, lower, n, b, P, Gd, Gu, Gl, ws);
+  SINVB_CUDA(cudaMemsetAsync(ws, 0, sizeof(WsHeader), stream));  // status and barrier; the reduction stays
+  T* bnd = (T*)boundary;
+  void* args[] = {(void*)&p, (void*)&part, (void*)&stage, (void*)&bnd};
+  if (b <= 32) return psr_launch<T>(psr_part_kernel<T, 32, 32>, args, 1, stream);
+  return psr_launch<T>(psr_part_kernel<T, 64, 64>, args, 1, stream);
 }
 
 }  // namespace
@@ -467,6 +547,20 @@ int sinvb_psr_d(const void* diag, const void* upper, const void* lower, int n, i
                 sinvb_stream_t stream) {
   return psr_run<double>(diag, upper, lower, n, b, partitions, flags, G_diag, G_upper, G_lower, workspace,
                          workspace_bytes, (cudaStream_t)stream);
+}
+
+int sinvb_psr_part_z(const void* diag, const void* upper, const void* lower, int n, int b, int partitions, int part,
+                     int stage, void* boundary, void* G_diag, void* G_upper, void* G_lower, void* workspace,
+                     size_t workspace_bytes, sinvb_stream_t stream) {
+  return psr_part_run<cplx>(diag, upper, lower, n, b, partitions, part, stage, boundary, G_diag, G_upper, G_lower,
+                            workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int sinvb_psr_part_d(const void* diag, const void* upper, const void* lower, int n, int b, int partitions, int part,
+                     int stage, void* boundary, void* G_diag, void* G_upper, void* G_lower, void* workspace,
+                     size_t workspace_bytes, sinvb_stream_t stream) {
+  return psr_part_run<double>(diag, upper, lower, n, b, partitions, part, stage, boundary, G_diag, G_upper, G_lower,
+                              workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
 }  // extern "C"
