@@ -265,17 +265,22 @@ int sinvb_psr_d(const void* diag, const void* upper, const void* lower, int n, i
                 sinvb_stream_t stream);
 /*
  * One partition of a multi-GPU PSR on this GPU: what reference process
- * ``part`` of ``partitions`` does (psr_seqsolve.py:52-70), every process
- * holding the whole block arrays.  stage 0 reduces the partition and writes
- * its part of the reduced system to ``boundary`` (4 b x b blocks, device):
- * first partition D[B]; last D[t]; central D[t], D[B], A[t,B], A[B,t] (t, B
- * the partition's first and last block rows).  stage 1 takes the boundary
- * blocks of the reduced system's inverse in the same slots (G[B,B]; G[t,t];
- * G[t,t], G[B,B], G[t,B], G[B,t]) and writes the partition's rows of G_diag /
- * G_upper / G_lower (the coupling to the next partition, G[B,B+1] and
- * G[B+1,B], comes from the reduced inverse and is the caller's to store).
- * Use the same workspace (sinvb_psr_workspace_size) for both stages.
+ * ``part`` of ``partitions`` does (psr_seqsolve.py:52-70), holding only its
+ * own block rows t .. B (m = B - t + 1 rows; the partitions are those of
+ * psr_utils.py:61-100).  diag: m blocks; upper / lower: the couplings
+ * A[i,i+1] / A[i+1,i] of rows t .. B (m blocks, m - 1 for the last partition);
+ * G_diag / G_upper / G_lower: the same shapes.  stage 0 reduces the partition
+ * and writes six b x b slots to ``boundary`` (device): its part of the
+ * reduced system (first partition D[B]; last D[t]; central D[t], D[B],
+ * A[t,B], A[B,t]) and in slots 4, 5 the couplings A[B,B+1], A[B+1,B] to the
+ * next partition (zero for the last).  stage 1 takes the boundary blocks of
+ * the reduced system's inverse in slots 0-3 (G[B,B]; G[t,t]; G[t,t], G[B,B],
+ * G[t,B], G[B,t]) and writes the partition's blocks; the couplings to the
+ * next partition, G[B,B+1] and G[B+1,B] (element m - 1 of G_upper /
+ * G_lower), come from the reduced inverse and are the caller's to store.
+ * Use one workspace of sinvb_psr_part_workspace_size bytes for both stages.
  */
+size_t sinvb_psr_part_workspace_size(int n, int b, int partitions, int part, int dtype);
 int sinvb_psr_part_z(const void* diag, const void* upper, const void* lower, int n, int b, int partitions, int part,
                      int stage, void* boundary, void* G_diag, void* G_upper, void* G_lower, void* workspace,
                      size_t workspace_bytes, sinvb_stream_t stream);

@@ -75,6 +75,7 @@ SIGNATURES = {
     "sinvb_psr_workspace_size": (_sz, [_i, _i, _i, _i, _u]),
     "sinvb_psr_z": (_i, [_vp, _vp, _vp, _i, _i, _i, _u, _vp, _vp, _vp, _vp, _sz, _vp]),
     "sinvb_psr_d": (_i, [_vp, _vp, _vp, _i, _i, _i, _u, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "sinvb_psr_part_workspace_size": (_sz, [_i, _i, _i, _i, _i]),
     "sinvb_psr_part_z": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "sinvb_psr_part_d": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "sinvb_bcr_batched_workspace_size": (_sz, [_vp, _i, _i, _u]),

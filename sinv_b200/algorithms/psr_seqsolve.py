@@ -103,24 +103,32 @@ def reduced_rows(n, P):
     return rows
 
 
-def reduced_system(boundaries, A_upper, A_lower, n, P):
-    """The block tridiagonal reduced system from every partition's boundary
-    slots (in partition order) and the input couplings between partitions.
-    Returns ``(R_diag, R_upper, R_lower)`` stacked like ``boundaries[0]``
-    (host bookkeeping on tensors of any device)."""
+def local_blocks(A_diag, A_upper, A_lower, partitions, part):
+    """The block arrays partition ``part`` holds: diag rows t..B and the
+    couplings of rows t..B (one fewer for the last partition)."""
+    n = A_diag.shape[0]
+    t, B = part_rows(n, partitions, part)
+    e = min(B + 1, n - 1)
+    return A_diag[t:B + 1], A_upper[t:e], A_lower[t:e]
+
+
+def reduced_system(boundaries, n, P):
+    """The block tridiagonal reduced system from every partition's six boundary
+    slots (in partition order): slots 0-3 its part of the reduced system, slots
+    4-5 its couplings to the next partition.  Returns ``(R_diag, R_upper,
+    R_lower)`` (host bookkeeping on tensors of any device)."""
     import torch
-    rows = reduced_rows(n, P)
     diag = [boundaries[0][0]]
     for p in range(1, P - 1):
         diag += [boundaries[p][0], boundaries[p][1]]
     diag.append(boundaries[P - 1][0])
     upper, lower = [], []
-    for x in range(len(rows) - 1):
-        if x % 2 == 0:  # B_p -> t_{p+1}: the input coupling
-            upper.append(A_upper[rows[x]])
-            lower.append(A_lower[rows[x]])
+    for x in range(2 * (P - 1) - 1):
+        p = (x + 1) // 2
+        if x % 2 == 0:  # B_p -> t_{p+1}: the input coupling sent by partition p
+            upper.append(boundaries[x // 2][4])
+            lower.append(boundaries[x // 2][5])
         else:           # t_p -> B_p of a central partition: its fill-in
-            p = (x + 1) // 2
             upper.append(boundaries[p][2])
             lower.append(boundaries[p][3])
     return torch.stack(diag), torch.stack(upper), torch.stack(lower)
@@ -145,36 +153,46 @@ def boundary_inverse(RG, part, P):
 
 
 class PsrPart:
-    """Partition ``part`` of a ``partitions``-way PSR on this GPU
-    (``sinvb_psr_part_*``): ``reduce()`` returns the boundary slots,
-    ``produce(slots, link)`` fills the partition's rows of G.  The block arrays
-    are the whole matrix, as every reference process holds it."""
+    """Partition ``part`` of a ``partitions``-way PSR of an n-block matrix on
+    this GPU (``sinvb_psr_part_*``), holding only the partition's rows
+    (``local_blocks``).  ``reduce()`` returns the six boundary slots,
+    ``produce(slots, link)`` returns the partition's ``(G_diag, G_upper,
+    G_lower)`` with the shapes of its local arrays (the last element of
+    G_upper / G_lower is the coupling to the next partition)."""
 
-    def __init__(self, A_diag, A_upper, A_lower, partitions, part, device=None):
+    def __init__(self, local_diag, local_upper, local_lower, n, partitions, part, device=None):
         torch = dev._torch()
         self.lib = _lib.load()
-        self.in_dt = dev.torch_dtype(A_diag)
+        self.in_dt = dev.torch_dtype(local_diag)
         self.wide = {torch.complex64: torch.complex128, torch.float32: torch.float64}.get(self.in_dt, self.in_dt)
         self.code = _lib.dtype_code(self.wide)
         if self.code not in (_lib.C128, _lib.F64):
             raise TypeError("unsupported dtype %s" % self.in_dt)
-        with torch.cuda.device(device if device is not None else torch.cuda.current_device()):
-            self.d = dev.to_device(A_diag, self.wide)
-            self.u = dev.to_device(A_upper, self.wide)
-            self.l = dev.to_device(A_lower, self.wide)
-        self.n, self.b = int(self.d.shape[0]), int(self.d.shape[1])
+        self.n = int(n)
         self.P = partitions_for(self.n, partitions)
         if self.P < 0 or not 0 <= part < self.P:
             raise ValueError("PSR needs 3 <= partitions <= 32, 3 block rows per partition and 0 <= part < "
                              "partitions (n=%d, partitions=%s, part=%d)" % (self.n, partitions, part))
         self.part = part
+        self.rows = part_rows(self.n, self.P, part)
+        m = self.rows[1] - self.rows[0] + 1
+        mc = m if part < self.P - 1 else m - 1
+        with torch.cuda.device(device if device is not None else torch.cuda.current_device()):
+            self.d = dev.to_device(local_diag, self.wide)
+            self.u = dev.to_device(local_upper, self.wide)
+            self.l = dev.to_device(local_lower, self.wide)
+        self.b = int(self.d.shape[-1])
+        b = self.b
+        for name, t, k in (("diag", self.d, m), ("upper", self.u, mc), ("lower", self.l, mc)):
+            if tuple(t.shape) != (k, b, b):
+                raise ValueError("partition %d: local %s must be (%d, %d, %d), got %s"
+                                 % (part, name, k, b, b, tuple(t.shape)))
         self.device = self.d.device
-        n, b = self.n, self.b
-        self.G = tuple(torch.zeros((m, b, b), dtype=self.wide, device=self.device) for m in (n, n - 1, n - 1))
-        self.slots = torch.zeros((4, b, b), dtype=self.wide, device=self.device)
+        self.G = tuple(torch.zeros((k, b, b), dtype=self.wide, device=self.device) for k in (m, mc, mc))
+        self.slots = torch.zeros((6, b, b), dtype=self.wide, device=self.device)
         with torch.cuda.device(self.device):
-            self.ws = dev.workspace(self.lib.sinvb_psr_workspace_size(n, b, self.P, self.code, 0), self.device)
-        self.rows = part_rows(n, self.P, part)
+            nbytes = self.lib.sinvb_psr_part_workspace_size(self.n, b, self.P, part, self.code)
+            self.ws = dev.workspace(nbytes, self.device)
 
     def _stage(self, stage, stream=None):
         torch = dev._torch()
@@ -190,12 +208,11 @@ class PsrPart:
         return self.slots
 
     def produce(self, slots, link=None, stream=None, check=True):
-        self.slots.copy_(slots)
+        self.slots[:4].copy_(slots[:4])
         self._stage(1, stream)
-        B = self.rows[1]
         if link is not None:
-            self.G[1][B].copy_(link[0])
-            self.G[2][B].copy_(link[1])
+            self.G[1][-1].copy_(link[0])
+            self.G[2][-1].copy_(link[1])
         if check:
             dev.raise_for_status(dev.read_status(self.lib, self.ws, stream), "psr part %d" % self.part)
         return self.G

@@ -72,6 +72,7 @@ struct PsrParams {
   WsHeader* hdr;
   int* status;
   int n, b, P;
+  int row0;  // global block row of element 0 of the row-indexed arrays (0 for a whole matrix)
 };
 
 // Partition k of n block rows over P (psr_utils.py:61-100): n / P rows each,
@@ -85,11 +86,13 @@ __host__ __device__ __forceinline__ int part_size(int n, int P, int k) {
   return k == 0 ? n - base * (P - 1) : base;
 }
 
+// Block of global row i in an array whose element 0 is global row row0.
 template <class T>
 struct Blk {
   T* base;
   size_t bb;
-  __device__ __forceinline__ T* operator()(int i) const { return base + (size_t)i * bb; }
+  int row0;
+  __device__ __forceinline__ T* operator()(int i) const { return base + (size_t)(i - row0) * bb; }
 };
 
 // C = -(A B + A2 B2) (+ D when given)
@@ -128,9 +131,11 @@ __device__ bool psr_reduce(Team& team, const PsrParams<T>& p, int part, T* side,
                            T* smem) {
   const int b = p.b, P = p.P, s = part_start(p.n, P, part), m = part_size(p.n, P, part);
   const size_t bb = (size_t)b * b;
-  const Blk<T> D{p.D, bb}, LA{p.LA, bb}, UA{p.UA, bb}, LT{p.LT, bb}, UT{p.UT, bb}, FR{p.FR, bb}, FC{p.FC, bb};
-  const Blk<const T> up{p.upper, bb}, lo{p.lower, bb};
-  team_copy<T>(team, m * b, b, p.diag + (size_t)s * bb, b, D(s), b);
+  const int r0 = p.row0;
+  const Blk<T> D{p.D, bb, r0}, LA{p.LA, bb, r0}, UA{p.UA, bb, r0}, LT{p.LT, bb, r0}, UT{p.UT, bb, r0},
+      FR{p.FR, bb, r0}, FC{p.FC, bb, r0};
+  const Blk<const T> up{p.upper, bb, r0}, lo{p.lower, bb, r0};
+  team_copy<T>(team, m * b, b, p.diag + (size_t)(s - r0) * bb, b, D(s), b);
   if (!team.sync()) return false;
   if (part == 0) {
     for (int i = s + 1; i < s + m; i++) {
@@ -183,8 +188,10 @@ template <class T, int BM, int BN, class Team>
 __device__ bool psr_produce(Team& team, const PsrParams<T>& p, int part, GemmOp<T>* ops, T* smem) {
   const int b = p.b, P = p.P, s = part_start(p.n, P, part), m = part_size(p.n, P, part);
   const size_t bb = (size_t)b * b;
-  const Blk<T> D{p.D, bb}, LA{p.LA, bb}, UA{p.UA, bb}, LT{p.LT, bb}, UT{p.UT, bb}, GR{p.GR, bb}, GC{p.GC, bb};
-  const Blk<T> Gd{p.Gd, bb}, Gu{p.Gu, bb}, Gl{p.Gl, bb};
+  const int r0 = p.row0;
+  const Blk<T> D{p.D, bb, r0}, LA{p.LA, bb, r0}, UA{p.UA, bb, r0}, LT{p.LT, bb, r0}, UT{p.UT, bb, r0},
+      GR{p.GR, bb, r0}, GC{p.GC, bb, r0};
+  const Blk<T> Gd{p.Gd, bb, r0}, Gu{p.Gu, bb, r0}, Gl{p.Gl, bb, r0};
   if (part == 0) {
     for (int i = s + m - 1; i > s; i--) {
       ops[0] = make_op<T>(b, b, b, -1.0, Gd(i), b, LA(i), b, nullptr, 0, Gl(i - 1), b);  // G[i,i-1]
@@ -248,7 +255,7 @@ template <class T, int BM, int BN, class Team>
 __device__ bool reduced_sweep(Team& all, const PsrParams<T>& p, int R, GemmOp<T>* ops, T* smem) {
   const int b = p.b;
   const size_t bb = (size_t)b * b;
-  const Blk<T> A{p.Rd, bb}, U{p.Ru, bb}, L{p.Rl, bb}, Gd{p.RGd, bb}, Gu{p.RGu, bb}, Gl{p.RGl, bb};
+  const Blk<T> A{p.Rd, bb, 0}, U{p.Ru, bb, 0}, L{p.Rl, bb, 0}, Gd{p.RGd, bb, 0}, Gu{p.RGu, bb, 0}, Gl{p.RGl, bb, 0};
   T* Winv = p.side + (size_t)p.P * p.side_elems;
   T* work = p.work + (size_t)p.P * 2 * bb;
   team_copy<T>(all, b, b, A(0), b, Gd(0), b);
@@ -348,23 +355,26 @@ struct PsrLayout {
   size_t bar, blocks, reduced, T0, work, side, total, side_elems;
 };
 
-PsrLayout psr_layout(int n, int b, int P, size_t es) {
+// rows: block rows the launch holds (n for a whole matrix, the partition's m
+// for one partition); teams: P for a whole matrix (with the reduced system on
+// the device), 1 for one partition.
+PsrLayout psr_layout(int rows, int b, int P, int teams, size_t es) {
   PsrLayout L{};
   const size_t bb = (size_t)b * b * es;
-  const int R = 2 * (P - 1);
+  const int R = teams > 1 ? 2 * (P - 1) : 0;
   size_t off = sizeof(WsHeader);
   auto take = [&](size_t bytes) {
     size_t at = off;
     off += align_up(bytes, 256);
     return at;
   };
-  L.bar = take((size_t)P * sizeof(unsigned));
-  L.blocks = take(9 * (size_t)n * bb);
-  L.reduced = take((size_t)(3 * R - 2) * 2 * bb);
+  L.bar = take((size_t)teams * sizeof(unsigned));
+  L.blocks = take(9 * (size_t)rows * bb);
+  L.reduced = take(R > 0 ? (size_t)(3 * R - 2) * 2 * bb : 0);
   L.T0 = take(bb);
-  L.work = take((size_t)(P + 1) * 2 * bb);
+  L.work = take((size_t)(teams + 1) * 2 * bb);
   L.side_elems = invert_side_elems(b);
-  L.side = take((size_t)(P + 1) * L.side_elems * es);
+  L.side = take((size_t)(teams + 1) * L.side_elems * es);
   L.total = off;
   return L;
 }
@@ -376,21 +386,23 @@ int psr_partitions(int n, int partitions) {
 }
 
 template <class T>
-int psr_check(const void* diag, const void* upper, const void* lower, int n, int b, int P, const void* Gd,
-              const void* Gu, const void* Gl, const void* workspace, size_t workspace_bytes) {
-  if (n < 1 || b < 1 || !diag || !upper || !lower || !Gd || !Gu || !Gl || !workspace) return SINVB_EINVAL;
-  if (P < 0) return SINVB_EINVAL;
-  for (const void* q : {diag, upper, lower, Gd, Gu, Gl})
-    if ((uintptr_t)q % sizeof(T)) return SINVB_EINVAL;
+int psr_check(const void* diag, const void* Gd, const void* const* others, int nothers, const void* workspace,
+              size_t workspace_bytes, size_t need) {
+  if (!diag || !Gd || !workspace) return SINVB_EINVAL;
+  if ((uintptr_t)diag % sizeof(T) || (uintptr_t)Gd % sizeof(T)) return SINVB_EINVAL;
+  for (int k = 0; k < nothers; k++)
+    if (others[k] && (uintptr_t)others[k] % sizeof(T)) return SINVB_EINVAL;
   if ((uintptr_t)workspace % 256) return SINVB_EWORKSPACE;
-  if (workspace_bytes < psr_layout(n, b, P, sizeof(T)).total) return SINVB_EWORKSPACE;
+  if (workspace_bytes < need) return SINVB_EWORKSPACE;
   return check_device();
 }
 
+// rows / row0: the block rows the arrays hold and the global row of their
+// first element; teams as in psr_layout.
 template <class T>
-PsrParams<T> psr_params(const void* diag, const void* upper, const void* lower, int n, int b, int P, void* Gd,
-                        void* Gu, void* Gl, unsigned char* ws) {
-  const PsrLayout L = psr_layout(n, b, P, sizeof(T));
+PsrParams<T> psr_params(const void* diag, const void* upper, const void* lower, int n, int b, int P, int rows,
+                        int row0, int teams, void* Gd, void* Gu, void* Gl, unsigned char* ws) {
+  const PsrLayout L = psr_layout(rows, b, P, teams, sizeof(T));
   const size_t bb = (size_t)b * b;
   PsrParams<T> p{};
   p.diag = (const T*)diag;
@@ -401,15 +413,17 @@ PsrParams<T> psr_params(const void* diag, const void* upper, const void* lower, 
   p.Gl = (T*)Gl;
   T* blk = reinterpret_cast<T*>(ws + L.blocks);
   T** arrays[9] = {&p.D, &p.LA, &p.UA, &p.LT, &p.UT, &p.FR, &p.FC, &p.GR, &p.GC};
-  for (int k = 0; k < 9; k++) *arrays[k] = blk + (size_t)k * n * bb;
-  const int R = 2 * (P - 1);
-  T* red = reinterpret_cast<T*>(ws + L.reduced);
-  p.Rd = red;
-  p.Ru = p.Rd + (size_t)R * bb;
-  p.Rl = p.Ru + (size_t)(R - 1) * bb;
-  p.RGd = p.Rl + (size_t)(R - 1) * bb;
-  p.RGu = p.RGd + (size_t)R * bb;
-  p.RGl = p.RGu + (size_t)(R - 1) * bb;
+  for (int k = 0; k < 9; k++) *arrays[k] = blk + (size_t)k * rows * bb;
+  if (teams > 1) {
+    const int R = 2 * (P - 1);
+    T* red = reinterpret_cast<T*>(ws + L.reduced);
+    p.Rd = red;
+    p.Ru = p.Rd + (size_t)R * bb;
+    p.Rl = p.Ru + (size_t)(R - 1) * bb;
+    p.RGd = p.Rl + (size_t)(R - 1) * bb;
+    p.RGu = p.RGd + (size_t)R * bb;
+    p.RGl = p.RGu + (size_t)(R - 1) * bb;
+  }
   p.T0 = reinterpret_cast<T*>(ws + L.T0);
   p.side = reinterpret_cast<T*>(ws + L.side);
   p.work = reinterpret_cast<T*>(ws + L.work);
@@ -420,6 +434,7 @@ PsrParams<T> psr_params(const void* diag, const void* upper, const void* lower, 
   p.n = n;
   p.b = b;
   p.P = P;
+  p.row0 = row0;
   return p;
 }
 
@@ -441,27 +456,34 @@ int psr_launch(Kern kern, void** args, int min_grid, cudaStream_t stream) {
 template <class T>
 int psr_run(const void* diag, const void* upper, const void* lower, int n, int b, int partitions, unsigned flags,
             void* Gd, void* Gu, void* Gl, void* workspace, size_t workspace_bytes, cudaStream_t stream) {
-  if (flags) return SINVB_EINVAL;
+  if (flags || n < 1 || b < 1) return SINVB_EINVAL;
   const int P = psr_partitions(n, partitions);
-  int rc = psr_check<T>(diag, upper, lower, n, b, P, Gd, Gu, Gl, workspace, workspace_bytes);
+  if (P < 0 || !upper || !lower || !Gu || !Gl) return SINVB_EINVAL;
+  const void* others[4] = {upper, lower, Gu, Gl};
+  const PsrLayout L = psr_layout(n, b, P, P, sizeof(T));
+  int rc = psr_check<T>(diag, Gd, others, 4, workspace, workspace_bytes, L.total);
   if (rc) return rc;
   unsigned char* ws = (unsigned char*)workspace;
-  PsrParams<T> p = psr_params<T>(diag, upper, lower, n, b, P, Gd, Gu, Gl, ws);
-  SINVB_CUDA(cudaMemsetAsync(ws, 0, psr_layout(n, b, P, sizeof(T)).blocks, stream));  // header, team barriers
+  PsrParams<T> p = psr_params<T>(diag, upper, lower, n, b, P, n, 0, P, Gd, Gu, Gl, ws);
+  SINVB_CUDA(cudaMemsetAsync(ws, 0, L.blocks, stream));  // header, team barriers
   void* args[] = {(void*)&p};
   if (b <= 32) return psr_launch<T>(psr_kernel<T, 32, 32>, args, P, stream);
   return psr_launch<T>(psr_kernel<T, 64, 64>, args, P, stream);
 }
 
+constexpr int kPsrSlots = 6;
+
 // One partition on its own GPU, the form a rank of a multi-GPU PSR runs
-// (psr_seqsolve.py:52-70 on process `part`), with the whole grid as the team.
-// stage 0 reduces the partition and writes its part of the reduced system to
-// four boundary slots (psr_seqsolve.py:387-467): first partition D[B]; last
-// D[t]; central D[t], D[B], A[t,B], A[B,t].  stage 1 reads the boundary
-// blocks of the inverse from the same slots (first G[B,B]; last G[t,t];
-// central G[t,t], G[B,B], G[t,B], G[B,t]; psr_seqsolve.py:564-644) and
-// produces the partition.  The workspace carries the reduction from stage 0
-// to stage 1.
+// (psr_seqsolve.py:52-70 on process `part`), with the whole grid as the team
+// and only the partition's rows t .. B in memory (local arrays, element 0 =
+// row t).  stage 0 reduces the partition and writes its part of the reduced
+// system to six boundary slots (psr_seqsolve.py:387-467): first partition
+// D[B]; last D[t]; central D[t], D[B], A[t,B], A[B,t]; and in slots 4, 5 the
+// couplings to the next partition A[B,B+1], A[B+1,B] (zero for the last).
+// stage 1 reads the boundary blocks of the inverse from slots 0-3 (first
+// G[B,B]; last G[t,t]; central G[t,t], G[B,B], G[t,B], G[B,t];
+// psr_seqsolve.py:564-644) and produces the partition.  The workspace carries
+// the reduction from stage 0 to stage 1.
 template <class T, int BM, int BN>
 __global__ void __launch_bounds__(kThreads, 1) psr_part_kernel(PsrParams<T> p, int part, int stage, T* bnd) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -469,50 +491,56 @@ __global__ void __launch_bounds__(kThreads, 1) psr_part_kernel(PsrParams<T> p, i
   const int P = p.P, b = p.b;
   const size_t bb = (size_t)b * b;
   const int t = part_start(p.n, P, part), B = t + part_size(p.n, P, part) - 1;
+  const size_t lt = (size_t)(t - p.row0) * bb, lB = (size_t)(B - p.row0) * bb;  // local offsets of rows t, B
   TeamDyn all{&p.hdr->barrier_count, p.status, (int)blockIdx.x, (int)gridDim.x, 0u};
   GemmOp<T> ops[4];
-  T* slot[4] = {bnd, bnd + bb, bnd + 2 * bb, bnd + 3 * bb};
   if (stage == 0) {
     if (!psr_reduce<T, BM, BN>(all, p, part, p.side, p.work, ops, smem)) return;
-    if (part == 0) {
-      team_copy<T>(all, b, b, p.D + (size_t)B * bb, b, slot[0], b);
-    } else if (part == P - 1) {
-      team_copy<T>(all, b, b, p.D + (size_t)t * bb, b, slot[0], b);
-    } else {
-      team_copy<T>(all, b, b, p.D + (size_t)t * bb, b, slot[0], b);
-      team_copy<T>(all, b, b, p.D + (size_t)B * bb, b, slot[1], b);
-      team_copy<T>(all, b, b, p.FR + (size_t)B * bb, b, slot[2], b);
-      team_copy<T>(all, b, b, p.FC + (size_t)B * bb, b, slot[3], b);
+    const bool central = part > 0 && part < P - 1;
+    team_copy<T>(all, b, b, p.D + (part == 0 ? lB : lt), b, bnd, b);
+    if (central) {
+      team_copy<T>(all, b, b, p.D + lB, b, bnd + bb, b);
+      team_copy<T>(all, b, b, p.FR + lB, b, bnd + 2 * bb, b);
+      team_copy<T>(all, b, b, p.FC + lB, b, bnd + 3 * bb, b);
+    }
+    if (part < P - 1) {
+      team_copy<T>(all, b, b, p.upper + lB, b, bnd + 4 * bb, b);
+      team_copy<T>(all, b, b, p.lower + lB, b, bnd + 5 * bb, b);
     }
     all.sync();
   } else {
-    if (part == 0) {
-      team_copy<T>(all, b, b, slot[0], b, p.Gd + (size_t)B * bb, b);
-    } else if (part == P - 1) {
-      team_copy<T>(all, b, b, slot[0], b, p.Gd + (size_t)t * bb, b);
-    } else {
-      team_copy<T>(all, b, b, slot[0], b, p.Gd + (size_t)t * bb, b);
-      team_copy<T>(all, b, b, slot[1], b, p.Gd + (size_t)B * bb, b);
-      team_copy<T>(all, b, b, slot[2], b, p.GR + (size_t)B * bb, b);
-      team_copy<T>(all, b, b, slot[3], b, p.GC + (size_t)B * bb, b);
+    const bool central = part > 0 && part < P - 1;
+    team_copy<T>(all, b, b, bnd, b, p.Gd + (part == 0 ? lB : lt), b);
+    if (central) {
+      team_copy<T>(all, b, b, bnd + bb, b, p.Gd + lB, b);
+      team_copy<T>(all, b, b, bnd + 2 * bb, b, p.GR + lB, b);
+      team_copy<T>(all, b, b, bnd + 3 * bb, b, p.GC + lB, b);
     }
     if (!all.sync()) return;
     psr_produce<T, BM, BN>(all, p, part, ops, smem);
   }
 }
 
+// diag: the partition's m diagonal blocks; upper / lower: its couplings
+// A[i,i+1] / A[i+1,i] for rows t .. B (m blocks; m - 1 for the last
+// partition, which has no next); G_diag / G_upper / G_lower likewise.
 template <class T>
 int psr_part_run(const void* diag, const void* upper, const void* lower, int n, int b, int partitions, int part,
                  int stage, void* boundary, void* Gd, void* Gu, void* Gl, void* workspace, size_t workspace_bytes,
                  cudaStream_t stream) {
+  if (n < 1 || b < 1) return SINVB_EINVAL;
   const int P = psr_partitions(n, partitions);
   if (P < 0 || part < 0 || part >= P || (stage != 0 && stage != 1) || !boundary) return SINVB_EINVAL;
-  if ((uintptr_t)boundary % sizeof(T)) return SINVB_EINVAL;
-  int rc = psr_check<T>(diag, upper, lower, n, b, P, Gd, Gu, Gl, workspace, workspace_bytes);
+  if (!upper || !lower || !Gu || !Gl) return SINVB_EINVAL;
+  const int m = part_size(n, P, part), t = part_start(n, P, part);
+  const void* others[5] = {upper, lower, Gu, Gl, boundary};
+  const PsrLayout L = psr_layout(m, b, P, 1, sizeof(T));
+  int rc = psr_check<T>(diag, Gd, others, 5, workspace, workspace_bytes, L.total);
   if (rc) return rc;
   unsigned char* ws = (unsigned char*)workspace;
-  PsrParams<T> p = psr_params<T>(diag, upper, lower, n, b, P, Gd, Gu, Gl, ws);
+  PsrParams<T> p = psr_params<T>(diag, upper, lower, n, b, P, m, t, 1, Gd, Gu, Gl, ws);
   SINVB_CUDA(cudaMemsetAsync(ws, 0, sizeof(WsHeader), stream));  // status and barrier; the reduction stays
+  if (stage == 0) SINVB_CUDA(cudaMemsetAsync(boundary, 0, kPsrSlots * (size_t)b * b * sizeof(T), stream));
   T* bnd = (T*)boundary;
   void* args[] = {(void*)&p, (void*)&part, (void*)&stage, (void*)&bnd};
   if (b <= 32) return psr_launch<T>(psr_part_kernel<T, 32, 32>, args, 1, stream);
@@ -532,7 +560,14 @@ size_t sinvb_psr_workspace_size(int n, int b, int partitions, int dtype, unsigne
   if (flags || b < 1 || (dtype != SINVB_C128 && dtype != SINVB_F64)) return 0;
   const int P = psr_partitions(n, partitions);
   if (P < 0) return 0;
-  return psr_layout(n, b, P, dtype == SINVB_C128 ? 16 : 8).total;
+  return psr_layout(n, b, P, P, dtype == SINVB_C128 ? 16 : 8).total;
+}
+
+size_t sinvb_psr_part_workspace_size(int n, int b, int partitions, int part, int dtype) {
+  if (b < 1 || (dtype != SINVB_C128 && dtype != SINVB_F64)) return 0;
+  const int P = psr_partitions(n, partitions);
+  if (P < 0 || part < 0 || part >= P) return 0;
+  return psr_layout(part_size(n, P, part), b, P, 1, dtype == SINVB_C128 ? 16 : 8).total;
 }
 
 int sinvb_psr_z(const void* diag, const void* upper, const void* lower, int n, int b, int partitions, unsigned flags,

@@ -125,57 +125,59 @@ def _gpu_energy_term(H_onsite, H_coupling, eta, sigma):
 
 
 # --------------------------------------------------------------------------- PSR across ranks
-def psr_distributed(A_diag, A_upper, A_lower, group=None, gather=True, make_part=None):
-    """Parallel Schur reduction with rank r of ``group`` as partition r, the
-    reference's process layout (``src/sinv/algorithms/psr/psr_seqsolve.py:20-73``;
-    at least 3 ranks and 3 block rows per rank, ``psr_utils.py:55-58``).
+def psr_distributed(local_diag, local_upper, local_lower, n, group=None, gather=False, make_part=None):
+    """Parallel Schur reduction of an n-block matrix with rank r of ``group`` as
+    partition r, the reference's process layout
+    (``src/sinv/algorithms/psr/psr_seqsolve.py:20-73``; at least 3 ranks and 3
+    block rows per rank, ``psr_utils.py:55-58``).
 
-    Every rank holds the whole block arrays, as every reference process holds A.
-    Each rank reduces its partition on its GPU (``PsrPart.reduce``), the four
-    boundary blocks of every partition cross ranks in one ``all_gather`` (the
-    reference's send / recv to rank 0, :313-467), every rank solves the small
-    reduced system itself (instead of rank 0 solving and sending back,
-    :470-645), and each rank produces its partition.  With ``gather`` the rows
-    of every partition are all-gathered so each rank returns the whole
-    ``(G_diag, G_upper, G_lower)`` (the reference aggregates on rank 0,
-    :903-943); otherwise each rank returns its own arrays, valid on its rows
-    (``PsrPart.rows``) and the coupling to the next partition.
+    Each rank passes only its partition's block arrays
+    (``psr_seqsolve.local_blocks(A_diag, A_upper, A_lower, world, rank)``), so
+    a matrix larger than one GPU's memory can be inverted; the reference's
+    processes each hold the whole A.  Each rank reduces its partition on its GPU
+    (``PsrPart.reduce``); the six boundary slots of every partition cross ranks
+    in one ``all_gather`` (the reference's send / recv to rank 0, :313-467);
+    every rank solves the small reduced system itself (instead of rank 0
+    solving and sending back, :470-645) and produces its partition.  Returns
+    this rank's ``(G_diag, G_upper, G_lower)`` in the shapes of its local
+    arrays, or with ``gather`` the whole arrays on every rank (the reference
+    aggregates on rank 0, :903-943).
 
     ``make_part`` builds the per-rank compute object (default: ``PsrPart`` on
-    the current GPU); it must provide ``n``, ``u``, ``l``, ``rows``,
-    ``reduce()``, ``solve_reduced(Rd, Ru, Rl)`` and ``produce(slots, link)``.
+    the current GPU); it must provide ``reduce()``, ``solve_reduced(Rd, Ru,
+    Rl)`` and ``produce(slots, link)``.
     """
     import torch
     from .algorithms import psr_seqsolve as psr
     dist = _dist()
     rank, world = rank_and_world(group)
-    part = make_part() if make_part is not None else psr.PsrPart(A_diag, A_upper, A_lower, world, rank)
+    part = make_part() if make_part is not None else psr.PsrPart(local_diag, local_upper, local_lower, n, world,
+                                                                  rank)
     slots = part.reduce().contiguous()
     if world > 1:
         every = [torch.empty_like(slots) for _ in range(world)]
         dist.all_gather(every, slots, group=group)
     else:
         every = [slots]
-    RG = part.solve_reduced(*psr.reduced_system(every, part.u, part.l, part.n, world))
+    RG = part.solve_reduced(*psr.reduced_system(every, n, world))
     gslots, link = psr.boundary_inverse(RG, rank, world)
     Gd, Gu, Gl = part.produce(gslots, link)
     if not gather:
         return Gd, Gu, Gl
-    n = part.n
     mmax = psr.part_rows(n, world, 0)[1] + 1  # the first partition is the largest
-    t, B = part.rows
-    e = min(B + 1, n - 1)
     buf = torch.zeros((3, mmax) + tuple(Gd.shape[1:]), dtype=Gd.dtype, device=Gd.device)
-    buf[0, :B + 1 - t] = Gd[t:B + 1]
-    buf[1, :e - t] = Gu[t:e]
-    buf[2, :e - t] = Gl[t:e]
+    buf[0, :Gd.shape[0]] = Gd
+    buf[1, :Gu.shape[0]] = Gu
+    buf[2, :Gl.shape[0]] = Gl
     pieces = [torch.empty_like(buf) for _ in range(world)] if world > 1 else [buf]
     if world > 1:
         dist.all_gather(pieces, buf, group=group)
+    shape = tuple(Gd.shape[1:])
+    out = [torch.empty((k,) + shape, dtype=Gd.dtype, device=Gd.device) for k in (n, n - 1, n - 1)]
     for r, pc in enumerate(pieces):
-        tr, Br = psr.part_rows(n, world, r)
-        er = min(Br + 1, n - 1)
-        Gd[tr:Br + 1] = pc[0, :Br + 1 - tr]
-        Gu[tr:er] = pc[1, :er - tr]
-        Gl[tr:er] = pc[2, :er - tr]
-    return Gd, Gu, Gl
+        t, B = psr.part_rows(n, world, r)
+        e = min(B + 1, n - 1)
+        out[0][t:B + 1] = pc[0, :B + 1 - t]
+        out[1][t:e] = pc[1, :e - t]
+        out[2][t:e] = pc[2, :e - t]
+    return tuple(out)

@@ -4,10 +4,10 @@
 
 Each rank's compute here is a stand-in built from the oracle's partition
 functions (test code only); on GPUs the same host logic drives ``PsrPart``
-(``sinvb_psr_part_*``).  What is under test: the boundary slots each rank
-contributes, the one all-gather, the reduced system every rank assembles and
-solves, the boundary blocks and coupling each rank takes back, and the final
-gather of the rows.  The result must equal the oracle PSR on the same
+(``sinvb_psr_part_*``).  Each rank passes only its partition's rows.  What is
+under test: the boundary slots each rank contributes, the one all-gather, the
+reduced system every rank assembles and solves, the boundary blocks and
+coupling each rank takes back, and the final gather of the rows.  The result must equal the oracle PSR on the same
 partitions and the dense inverse.
 """
 
@@ -25,7 +25,9 @@ from sinv_b200 import distributed, workloads
 
 
 class OraclePart:
-    """The per-rank compute of ``psr_distributed`` on the CPU, from the oracle."""
+    """The per-rank compute of ``psr_distributed`` on the CPU, from the oracle
+    (it reads the whole matrix, test code only; the slots and outputs follow
+    the ``PsrPart`` contract)."""
 
     def __init__(self, d, u, l, P, part):
         self.dn, self.un, self.ln = d, u, l
@@ -52,7 +54,8 @@ class OraclePart:
             slots = [self.A[(t, t)], z, z, z]
         else:
             slots = [self.A[(t, t)], self.A[(B, B)], self.A[(t, B)], self.A[(B, t)]]
-        return torch.from_numpy(np.stack(slots))
+        link = [self.un[B], self.ln[B]] if self.part < self.P - 1 else [z, z]
+        return torch.from_numpy(np.stack(slots + link))
 
     def solve_reduced(self, Rd, Ru, Rl):
         return tuple(torch.from_numpy(x) for x in rgf_oracle.rgf(Rd.numpy(), Ru.numpy(), Rl.numpy()))
@@ -69,16 +72,18 @@ class OraclePart:
             G[(t, t)], G[(B, B)], G[(t, B)], G[(B, t)] = sl[0], sl[1], sl[2], sl[3]
         f = self._kind(psr_oracle.produce_topleft, psr_oracle.produce_central, psr_oracle.produce_bottomright)
         f(self.A, self.L, self.U, self.Dinv, G, self.s, self.m)
-        n, b = self.n, self.b
-        Gd = np.zeros((n, b, b), self.dn.dtype)
-        Gu = np.zeros((n - 1, b, b), self.dn.dtype)
-        Gl = np.zeros((n - 1, b, b), self.dn.dtype)
+        b = self.b
+        m = B - t + 1
+        mc = m if self.part < self.P - 1 else m - 1
+        Gd = np.zeros((m, b, b), self.dn.dtype)
+        Gu = np.zeros((mc, b, b), self.dn.dtype)
+        Gl = np.zeros((mc, b, b), self.dn.dtype)
         for i in range(t, B + 1):
-            Gd[i] = G[(i, i)]
+            Gd[i - t] = G[(i, i)]
             if i < B:
-                Gu[i], Gl[i] = G[(i, i + 1)], G[(i + 1, i)]
+                Gu[i - t], Gl[i - t] = G[(i, i + 1)], G[(i + 1, i)]
         if link is not None:
-            Gu[B], Gl[B] = link[0].numpy(), link[1].numpy()
+            Gu[m - 1], Gl[m - 1] = link[0].numpy(), link[1].numpy()
         return torch.from_numpy(Gd), torch.from_numpy(Gu), torch.from_numpy(Gl)
 
 
@@ -93,8 +98,10 @@ def _rank_main(rank, world, port, out_dir, n, b, gather):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
+        from sinv_b200.algorithms.psr_seqsolve import local_blocks
         d, u, l = workloads.dominant(n, b, seed=n + b)
-        G = distributed.psr_distributed(d, u, l, gather=gather,
+        ld, lu, ll = local_blocks(d, u, l, world, rank)
+        G = distributed.psr_distributed(ld, lu, ll, n, gather=gather,
                                         make_part=lambda: OraclePart(d, u, l, world, rank))
         np.savez(os.path.join(out_dir, "r%d.npz" % rank), *[g.numpy() for g in G])
     finally:
@@ -125,7 +132,7 @@ def test_psr_ranks_without_gather_own_their_rows(tmp_path):
         z = np.load(os.path.join(tmp_path, "r%d.npz" % r))
         t, B = starts[r], starts[r] + sizes[r] - 1
         e = min(B + 1, n - 1)
-        assert dense.rel_fro(z["arr_0"][t:B + 1], R[0][t:B + 1]) <= 1e-13
-        assert dense.rel_fro(z["arr_1"][t:e], R[1][t:e]) <= 1e-13
-        assert dense.rel_fro(z["arr_2"][t:e], R[2][t:e]) <= 1e-13
-        assert not np.any(z["arr_0"][:t]) and not np.any(z["arr_0"][B + 1:])
+        assert z["arr_0"].shape[0] == B + 1 - t and z["arr_1"].shape[0] == e - t
+        assert dense.rel_fro(z["arr_0"], R[0][t:B + 1]) <= 1e-13
+        assert dense.rel_fro(z["arr_1"], R[1][t:e]) <= 1e-13
+        assert dense.rel_fro(z["arr_2"], R[2][t:e]) <= 1e-13

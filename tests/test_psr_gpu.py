@@ -106,20 +106,21 @@ def test_torch_inputs_single_precision_and_dense_torch():
                                          (64, 130, 6, np.complex128)])
 def test_partitions_one_at_a_time_as_ranks(n, b, P, dtype):
     """The per-rank path of a multi-GPU PSR (``sinvb_psr_part_*``), its ranks run
-    one after another on this GPU: each partition reduces, the boundary slots
-    are exchanged in-process (what the all-gather does across GPUs), the
-    reduced system is solved, each partition produces its rows."""
+    one after another on this GPU, each holding only its partition's rows:
+    each partition reduces, the boundary slots are exchanged in-process (what
+    the all-gather does across GPUs), the reduced system is solved, each
+    partition produces its rows."""
     d, u, l = workloads.dominant(n, b, seed=3 * n + b, dtype=dtype)
-    parts = [psr_s.PsrPart(d, u, l, P, k) for k in range(P)]
+    parts = [psr_s.PsrPart(*psr_s.local_blocks(d, u, l, P, k), n, P, k) for k in range(P)]
     slots = [p.reduce().clone() for p in parts]
-    RG = parts[0].solve_reduced(*psr_s.reduced_system(slots, parts[0].u, parts[0].l, n, P))
+    RG = parts[0].solve_reduced(*psr_s.reduced_system(slots, n, P))
     Gd, Gu, Gl = (np.zeros_like(x) for x in (d, u, l))
     for k, p in enumerate(parts):
         gs, link = psr_s.boundary_inverse(RG, k, P)
         G = [g.cpu().numpy() for g in p.produce(gs, link)]
         t, B = p.rows
         e = min(B + 1, n - 1)
-        Gd[t:B + 1], Gu[t:e], Gl[t:e] = G[0][t:B + 1], G[1][t:e], G[2][t:e]
+        Gd[t:B + 1], Gu[t:e], Gl[t:e] = G[0], G[1], G[2]
     R = psr_oracle.psr(d, u, l, P)
     assert _worst([Gd, Gu, Gl], R) <= 1e-12
     assert _worst([Gd, Gu, Gl], rgf_oracle.rgf(d, u, l)) <= 1e-12
