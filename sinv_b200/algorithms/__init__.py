@@ -19,4 +19,4 @@ from .batched import BatchPlan, rgf_batched, rgf_batched_host  # noqa: F401
 from . import adjoint  # noqa: F401
 from .adjoint import RGFFunction, rgf_autograd  # noqa: F401
 from . import lesser  # noqa: F401
-from .lesser import rgf_lesser  # noqa: F401
+from .lesser import rgf_greater, rgf_lesser  # noqa: F401

@@ -5,6 +5,7 @@ No reference counterpart: in a transport code this is the step after ``rgf``
 lesser self-energy Sigma< of the contacts (block-diagonal).  One sweep pair
 (``sinvb_rgf_lesser_z``) gives the retarded blocks of ``rgf`` and the lesser
 blocks G<_ii, G<_{i,i+1}; G<_{i+1,i} = -(G<_{i,i+1})^H (G< is anti-Hermitian).
+``rgf_greater`` is the same computation for the greater self-energy.
 """
 
 import numpy as np
@@ -44,3 +45,16 @@ def rgf_lesser(A_diag, A_upper, A_lower, Sigma_lesser, team=None, check=True, st
     Gd, Gu, Gl, GLd, GLu = out
     GLl = -GLu.conj().transpose(1, 2).contiguous()
     return tuple(dev.to_output(t, A_diag) for t in (Gd, Gu, Gl, GLd, GLu, GLl))
+
+
+def rgf_greater(A_diag, A_upper, A_lower, Sigma_greater, team=None, check=True, stream=None):
+    """``(A blocks, Sigma>_ii blocks) -> (G_diag, G_upper, G_lower, GG_diag, GG_upper, GG_lower)``:
+    the greater Green's function G> = G Sigma> G^H on the tridiagonal blocks.
+
+    Sigma> is anti-Hermitian like Sigma< (both are i times a Hermitian
+    broadening), and the recursions of ``rgf_lesser`` use nothing else about
+    the self-energy, so the same sweep pair computes G>; GG_lower is
+    -(GG_upper)^H.  With Sigma> - Sigma< = Sigma^R - Sigma^A the results obey
+    G> - G< = G - G^H.
+    """
+    return rgf_lesser(A_diag, A_upper, A_lower, Sigma_greater, team=team, check=check, stream=stream)

@@ -11,7 +11,7 @@ import pytest
 
 from oracle import dense, rgf_oracle
 from sinv_b200 import workloads
-from sinv_b200.algorithms import rgf_lesser
+from sinv_b200.algorithms import rgf_greater, rgf_lesser
 
 pytestmark = pytest.mark.gpu
 
@@ -67,3 +67,25 @@ def test_lesser_dominant_and_torch():
     Rd, Ru, _ = _dense_lesser(d, u, l, s)
     assert _worst([t.cpu().numpy() for t in out[3]], Rd) <= 1e-12
     assert _worst([t.cpu().numpy() for t in out[4]], Ru) <= 1e-12
+
+
+@pytest.mark.parametrize("n,b,E", [(6, 16, 0.2), (9, 64, -0.7), (4, 130, 1.1)])
+def test_greater_minus_lesser_is_spectral(n, b, E):
+    """Sigma< = i f Gamma, Sigma> = -i (1 - f) Gamma with Gamma = i (Sigma^R - Sigma^A)
+    (the eta broadening everywhere plus the contact blocks of the tight-binding
+    model): then G> - G< = G (Sigma^R - Sigma^A) G^H = G - G^H, blockwise."""
+    d, u, l = workloads.tight_binding(n, b, E, seed=n * b)
+    eye = np.eye(b)
+    gamma = np.stack([2 * workloads.ETA * eye + (2 * workloads.SIGMA_EDGE * eye if i in (0, n - 1) else 0)
+                      for i in range(n)]).astype(np.complex128)
+    f = 0.3
+    sl = 1j * f * gamma
+    sg = -1j * (1 - f) * gamma
+    Gd, Gu, Gl, Ld, Lu, Ll = rgf_lesser(d, u, l, sl)
+    _, _, _, Hd, Hu, Hl = rgf_greater(d, u, l, sg)
+    Rd, Ru, Rl = _dense_lesser(d, u, l, sg)
+    assert _worst(Hd, Rd) <= 1e-11 and _worst(Hu, Ru) <= 1e-11 and _worst(Hl, Rl) <= 1e-11
+    spec_d = Gd - np.conj(np.transpose(Gd, (0, 2, 1)))
+    spec_u = Gu - np.conj(np.transpose(Gl, (0, 2, 1)))
+    assert _worst([Hd - Ld], [spec_d]) <= 1e-10
+    assert _worst([Hu - Lu], [spec_u]) <= 1e-10
