@@ -4,11 +4,14 @@ Run from the repository root, with the reference sources available::
 
     python tests/golden/make_golden.py /path/to/reference         # rgf, bcr
     python tests/golden/make_golden.py /path/to/reference --psr   # psr_outputs.npz
+    python tests/golden/make_golden.py /path/to/reference --pdiv  # pdiv_outputs.npz
 
 ``psr_seqsolve`` (``src/sinv/algorithms/psr/psr_seqsolve.py:20-73``) needs at
 least three MPI processes; it runs here on P threads that exchange its
 ``send`` / ``recv`` messages through queues (``ThreadComm``), each thread on
-its own copy of the matrix as each MPI process has.
+its own copy of the matrix as each MPI process has.  ``pdiv_localmap``
+(``src/sinv/algorithms/pdiv/pdiv_localmap.py:27-91``, power-of-two process
+counts) runs the same way, each thread given its partition and the bridges.
 
 The reference ``rgf`` (``src/sinv/algorithms/rgf/rgf.py:17-64``) and
 ``bcr_serial`` (``src/sinv/algorithms/bcr/bcr_serial.py:19-62``) are imported
@@ -148,14 +151,21 @@ PSR_VARIANTS = [(True, False), (False, True)]
 
 class ThreadComm:
     """Point-to-point stand-in for ``MPI.COMM_WORLD`` over P threads: ``send`` /
-    ``recv`` by (source, dest, tag) queues, the rank from a thread-local."""
+    ``recv`` through one FIFO queue per (source, dest, tag), which is MPI's
+    matching rule for blocking point-to-point messages; the rank comes from a
+    thread-local."""
 
     def __init__(self, size):
-        import queue
         import threading
         self.size = size
         self.local = threading.local()
-        self.q = {(s, d): queue.Queue() for s in range(size) for d in range(size)}
+        self.lock = threading.Lock()
+        self.q = {}
+
+    def _queue(self, key):
+        import queue
+        with self.lock:
+            return self.q.setdefault(key, queue.Queue())
 
     def Get_rank(self):
         return self.local.rank
@@ -164,10 +174,10 @@ class ThreadComm:
         return self.size
 
     def send(self, obj, dest, tag=0):
-        self.q[(self.local.rank, dest)].put(np.array(obj, copy=True))
+        self._queue((self.local.rank, dest, tag)).put(np.array(obj, copy=True))
 
     def recv(self, source, tag=0):
-        return self.q[(source, self.local.rank)].get(timeout=600)
+        return self._queue((source, self.local.rank, tag)).get(timeout=600)
 
 
 def run_psr_reference(psr_mod, A, b, P):
@@ -222,10 +232,84 @@ def main_psr(ref_root):
     print("wrote", path, os.path.getsize(path), "bytes,", len(out), "arrays")
 
 
+# PDIV fixtures: the reference test's sizes (tests/pdiv_tests/pdiv_test.py:45-56)
+# on 2, 4 and 8 processes (powers of two, at most one per block).
+PDIV_SIZES = [(2, 1), (4, 2), (6, 3), (3, 1), (6, 2), (9, 3), (128, 8), (128, 16), (128, 32)]
+PDIV_VARIANTS = [(True, False), (False, True)]
+
+
+def run_pdiv_reference(pdiv_mod, pdiv_u, A, b, P):
+    """The reference ``pdiv_localmap`` (``pdiv_localmap.py:27-91``) on P threads,
+    each given its partition and the bridges as ``tests/pdiv_tests/pdiv_test.py:84-88``
+    does; returns the assembled (G_diag, G_upper, G_lower)."""
+    import threading
+    comm = ThreadComm(P)
+    pdiv_mod.MPI.COMM_WORLD = comm
+    starts, sizes = pdiv_u.divide_matrix(A, P, b)
+    K_i, Bu_i, Bl_i = pdiv_u.partition_subdomain(A, starts, sizes, b)
+    out, errs = {}, []
+
+    def rank(r):
+        comm.local.rank = r
+        try:
+            out[r] = pdiv_mod.pdiv_localmap(K_i[r].copy(), Bu_i, Bl_i, b)
+        except Exception as e:  # surfaced below
+            errs.append(e)
+
+    ts = [threading.Thread(target=rank, args=(r,)) for r in range(P)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    if errs:
+        raise errs[0]
+    n = A.shape[0] // b
+    Gd = np.zeros((n, b, b), A.dtype)
+    Gu = np.zeros((n - 1, b, b), A.dtype)
+    Gl = np.zeros((n - 1, b, b), A.dtype)
+    for r in range(P):
+        X_d, X_u, X_l = out[r]
+        for i in range(sizes[r]):
+            Gd[starts[r] + i] = X_d[i]
+            if starts[r] + i < n - 1:
+                Gu[starts[r] + i] = X_u[i]
+                Gl[starts[r] + i] = X_l[i]
+    return Gd, Gu, Gl
+
+
+def main_pdiv(ref_root):
+    import_reference(ref_root)  # the same mpi4py / quasi shims as main()
+    from sinv.algorithms.pdiv import pdiv_localmap as pdiv_mod
+    from sinv.algorithms.pdiv import pdiv_utils as pdiv_u
+    pdiv_u.MPI.COMM_WORLD = None
+    out = {}
+    for cplx, sym in PDIV_VARIANTS:
+        for N, b in PDIV_SIZES:
+            for P in (2, 4, 8):
+                if N // b < P:
+                    continue
+                A, _ = banded_case(N, b, cplx, sym)
+                G = run_pdiv_reference(pdiv_mod, pdiv_u, A, b, P)
+                key = f"pdiv_c{int(cplx)}_s{int(sym)}_N{N}_b{b}_P{P}"
+                out[key + "_in"] = checksum(A)
+                out[key + "_d"], out[key + "_u"], out[key + "_l"] = G
+    d, u, l = workloads.dominant(16, 12, seed=0)
+    Ad = matu.convertBlkTridiagToDense(d, u, l)
+    out["dom_pdiv_in"] = checksum(d, u, l)
+    for P in (2, 4, 8, 16):
+        out[f"dom_pdiv_P{P}_d"], out[f"dom_pdiv_P{P}_u"], out[f"dom_pdiv_P{P}_l"] = \
+            run_pdiv_reference(pdiv_mod, pdiv_u, Ad, 12, P)
+    path = os.path.join(HERE, "pdiv_outputs.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes,", len(out), "arrays")
+
+
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     root = args[0] if args else "/root/reference"
     if "--psr" in sys.argv:
         main_psr(root)
+    elif "--pdiv" in sys.argv:
+        main_pdiv(root)
     else:
         main(root)
