@@ -86,3 +86,46 @@ def test_product_path_has_no_cpu_fallback(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "_lib", None)
     with pytest.raises(_lib.SinvbUnavailable):
         _lib.load(str(tmp_path / "missing.so"))
+
+
+def test_psr_partition_rule_and_sizes(lib):
+    # sinvb_psr_partitions: about sqrt(n/2), 3 <= P <= 32, n >= 3P (psr_utils.py:55-58)
+    assert lib.sinvb_psr_partitions(64, 0) == 6
+    assert lib.sinvb_psr_partitions(9, 0) == 3
+    assert lib.sinvb_psr_partitions(2000, 0) == 32
+    assert lib.sinvb_psr_partitions(8, 0) == -1
+    assert lib.sinvb_psr_partitions(12, 4) == 4
+    assert lib.sinvb_psr_partitions(12, 5) == -1 and lib.sinvb_psr_partitions(12, 2) == -1
+    whole = lib.sinvb_psr_workspace_size(64, 256, 6, _lib.C128, 0)
+    parts = [lib.sinvb_psr_part_workspace_size(64, 256, 6, k, _lib.C128) for k in range(6)]
+    assert whole % 256 == 0 and all(p % 256 == 0 and p > 0 for p in parts)
+    assert max(parts) < whole / 4            # a rank holds only its partition's rows
+    assert parts[0] > parts[1] == parts[5]   # the first partition takes the remainder rows
+    assert lib.sinvb_psr_workspace_size(64, 256, 6, _lib.C128, 1) == 0   # flags must be 0
+    assert lib.sinvb_psr_part_workspace_size(64, 256, 6, 6, _lib.C128) == 0
+    assert lib.sinvb_psr_workspace_size(64, 256, 6, _lib.F64, 0) < whole
+
+
+def test_psr_and_bcr_batched_host_checks(lib):
+    buf = (ctypes.c_char * 4096)()
+    p = ctypes.cast(buf, ctypes.c_void_p)
+    null = None
+    assert lib.sinvb_psr_z(null, p, p, 12, 4, 3, 0, p, p, p, p, 4096, null) == _lib.EINVAL
+    assert lib.sinvb_psr_z(p, p, p, 12, 4, 5, 0, p, p, p, p, 4096, null) == _lib.EINVAL    # 12 < 3 * 5
+    assert lib.sinvb_psr_z(p, p, p, 12, 4, 3, 1, p, p, p, p, 4096, null) == _lib.EINVAL    # flags
+    assert lib.sinvb_psr_part_z(p, p, p, 12, 4, 3, 0, 2, p, p, p, p, p, 4096, null) == _lib.EINVAL  # stage
+    assert lib.sinvb_psr_part_z(p, p, p, 12, 4, 3, 3, 0, p, p, p, p, p, 4096, null) == _lib.EINVAL  # part
+    assert lib.sinvb_psr_part_z(p, p, p, 12, 4, 3, 0, 0, null, p, p, p, p, 4096, null) == _lib.EINVAL
+    descs = (_lib.BatchDesc * 2)()
+    descs[0] = _lib.BatchDesc(None, None, None, None, None, None, 3, 8)
+    descs[1] = _lib.BatchDesc(None, None, None, None, None, None, 0, 8)
+    cd = ctypes.cast(descs, ctypes.c_void_p)
+    assert lib.sinvb_bcr_batched_workspace_size(cd, 2, _lib.C128, 0) == 0     # n < 1
+    assert lib.sinvb_bcr_batched_workspace_size(cd, 1, _lib.C128, 0) > 0
+    assert lib.sinvb_bcr_batched_workspace_size(cd, 0, _lib.C128, 0) == 256  # the header alone
+    big = (ctypes.c_char * 8192)()
+    aligned = ctypes.c_void_p((ctypes.addressof(big) + 255) & ~255)   # workspaces are 256-byte aligned
+    assert lib.sinvb_bcr_batched_z(cd, 1, 0, aligned, 4096, null, null) == _lib.EINVAL   # null block pointers
+    assert lib.sinvb_bcr_batched_z(cd, -1, 0, aligned, 4096, null, null) == _lib.EINVAL
+    assert lib.sinvb_bcr_batched_z(cd, 1, 0, p if ctypes.addressof(buf) % 256 else None, 4096, null,
+                                   null) in (_lib.EINVAL, _lib.EWORKSPACE)
