@@ -14,6 +14,12 @@ reference's number of processes becomes ``partitions`` (None: about
 sqrt(n/2)).  ``psr_blocks`` is the block-array form.  The reference's limits
 hold: at least 3 partitions and 3 block rows per partition
 (``psr_utils.py:55-58``), raised as ``ValueError``.
+
+For one partition per GPU (the reference's one partition per process),
+``PsrPart`` runs a partition on this GPU holding only its rows
+(``local_blocks``), ``reduced_system`` / ``boundary_inverse`` do the host
+bookkeeping of the exchange, and ``sinv_b200.distributed.psr_distributed``
+drives them across ranks with one all-gather.
 """
 
 import numpy as np
