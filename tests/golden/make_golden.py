@@ -6,6 +6,9 @@ Run from the repository root, with the reference sources available::
     python tests/golden/make_golden.py /path/to/reference --psr   # psr_outputs.npz
     python tests/golden/make_golden.py /path/to/reference --pdiv  # pdiv_outputs.npz
 
+The reference root may also come from the ``SINV_REFERENCE`` environment
+variable; there is no default.
+
 ``psr_seqsolve`` (``src/sinv/algorithms/psr/psr_seqsolve.py:20-73``) needs at
 least three MPI processes; it runs here on P threads that exchange its
 ``send`` / ``recv`` messages through queues (``ThreadComm``), each thread on
@@ -306,7 +309,9 @@ def main_pdiv(ref_root):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    root = args[0] if args else "/root/reference"
+    root = args[0] if args else os.environ.get("SINV_REFERENCE")
+    if not root:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT [--psr|--pdiv] (or set SINV_REFERENCE)")
     if "--psr" in sys.argv:
         main_psr(root)
     elif "--pdiv" in sys.argv:

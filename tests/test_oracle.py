@@ -111,9 +111,9 @@ def test_matu_generators_follow_reference_seed_semantics():
 def test_against_live_reference_when_present():
     """Re-run the pin against the reference sources themselves (this container only)."""
     import os
-    ref = os.environ.get("SINV_REFERENCE", "/root/reference")
-    if not os.path.isdir(os.path.join(ref, "src", "sinv")):
-        pytest.skip("reference sources not present")
+    ref = os.environ.get("SINV_REFERENCE")
+    if not ref or not os.path.isdir(os.path.join(ref, "src", "sinv")):
+        pytest.skip("SINV_REFERENCE does not name the reference sources")
     from tests.golden import make_golden
     rgf_mod, bcr_mod = make_golden.import_reference(ref)
     d, u, l = workloads.dominant(6, 5, seed=11)
