@@ -241,6 +241,16 @@ int sinvb_rgf_batched_stream_d(const sinvb_batch_desc* descs, int count, unsigne
  */
 int sinvb_rgf_batched_rerun_z(void* workspace, sinvb_stream_t stream);
 int sinvb_rgf_batched_rerun_d(void* workspace, sinvb_stream_t stream);
+/*
+ * No reference counterpart (the reference has no device waits; its failure
+ * analogue is LinAlgError from rgf.py:44,48).  Bound, in seconds, of every
+ * device-side wait of the batched launches that use ``workspace`` from now
+ * on: team barriers, scratch slots and streamed ready words (default 60 s).
+ * A wait that reaches it reports SINVB_STATUS_TIMEOUT for its instance,
+ * which is then abandoned, and the launch goes on with the others.  Host-side
+ * setting, kept per workspace address; 0 < seconds <= 3600.
+ */
+int sinvb_rgf_batched_set_wait_limit(const void* workspace, double seconds);
 
 /* ---- PSR: parallel Schur reduction over partitions of one matrix -------------- */
 /*
@@ -339,17 +349,19 @@ int sinvb_fp64_mma_peak(int iters, double* tflops, sinvb_stream_t stream);
 /* ---- allocation-free variant ------------------------------------------------ */
 /*
  * No counterpart in the reference.  For callers that cannot allocate device
- * memory when they call (inside a stream capture whose graph must hold no
- * allocation nodes, inside an allocator hook or host callback, or in a
- * plugin whose host application owns all device memory): the single-matrix
- * complex128 RGF of sinvb_rgf_z with the scratch in a static device array
- * owned by the library (131,328 bytes, held by every GPU that loads the
- * library until exit), so only inputs and outputs are passed.
+ * memory when they call (inside an allocator hook or host callback that must
+ * not re-enter the allocator, or in a plugin whose host application owns all
+ * device memory): the single-matrix complex128 RGF of sinvb_rgf_z with the
+ * scratch in a static device array owned by the library (131,328 bytes, held
+ * by every GPU that loads the library until exit), so only inputs and
+ * outputs are passed.
  * Limits: b <= 64; SINVB_SAVE_OFFDIAG required when n > 1; flags other than
- * SINVB_SYM / SINVB_SAVE_OFFDIAG rejected (SINVB_EINVAL).  ``status``
+ * SINVB_SYM / SINVB_SAVE_OFFDIAG rejected (SINVB_EINVAL); output arrays that
+ * overlap an input or each other rejected (SINVB_EINVAL).  ``status``
  * (optional, device, one int) receives the device status.  The first call on
- * a device looks up the array's address: make it before any stream capture.
- * All calls share the array, so calls that overlap on the GPU race.
+ * a device does its set-up (the array's address, the kernels' shared-memory
+ * attributes): make it before any stream capture.  All calls share the
+ * array, so calls that overlap on the GPU race.
  */
 int sinvb_rgf_z_noalloc(const void* diag, const void* upper, const void* lower, int n, int b,
                         unsigned flags, void* G_diag, void* G_upper, void* G_lower, int* status,

@@ -57,6 +57,7 @@ SIGNATURES = {
     "sinvb_rgf_batched_stream_d": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp, _vp, _u, _vp]),
     "sinvb_rgf_batched_rerun_z": (_i, [_vp, _vp]),
     "sinvb_rgf_batched_rerun_d": (_i, [_vp, _vp]),
+    "sinvb_rgf_batched_set_wait_limit": (_i, [_vp, ctypes.c_double]),
     "sinvb_rgf_z_noalloc": (_i, [_vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _vp]),
     "sinvb_rgf_checkpoints": (_i, [_i, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "sinvb_rgf_forward_ckpt_z": (_i, [_vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _i, _vp, _sz, _vp]),

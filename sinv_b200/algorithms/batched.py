@@ -34,6 +34,11 @@ class BatchPlan:
     allocating one when it is large enough (``workspace_bytes``); plans that
     share one must run in order on one stream.
 
+    ``wait_limit`` (seconds, optional): bound of every device-side wait of
+    this plan's launches (team barriers, scratch slots, streamed ready
+    words; default 60 s).  An instance whose wait runs out gets status
+    ``STATUS_TIMEOUT`` and is abandoned; the launch finishes the others.
+
     ``precision="mixed"`` (complex128 only) computes the block products of
     both sweeps on the int8 tensor cores (Ozaki splitting into ``digits``
     int8 slices, exact int32 accumulation, FP64 reconstruction) and keeps
@@ -45,7 +50,7 @@ class BatchPlan:
     """
 
     def __init__(self, instances, sym_mat=False, save_off_diag=True, precision="fp64", outputs=None,
-                 device=None, inplace=False, team=None, digits=7, workspace=None):
+                 device=None, inplace=False, team=None, digits=7, workspace=None, wait_limit=None):
         torch = dev._torch()
         self.lib = _lib.load()
         if len(instances) == 0:
@@ -118,6 +123,13 @@ class BatchPlan:
                 self.ws = dev.workspace(nbytes, self.device)
             self.status_dev = torch.zeros(len(descs), dtype=torch.int32, device=self.device)
         self.uploaded = False
+        if wait_limit is not None:
+            self.set_wait_limit(wait_limit)
+
+    def set_wait_limit(self, seconds):
+        """Bound (seconds) of every device wait of this plan's later launches."""
+        _lib.check(self.lib.sinvb_rgf_batched_set_wait_limit(dev.ptr(self.ws), float(seconds)),
+                   "sinvb_rgf_batched_set_wait_limit")
 
     @staticmethod
     def workspace_bytes(shapes, dtype_code=None, flags=None, sym_mat=False, save_off_diag=True, precision="fp64",

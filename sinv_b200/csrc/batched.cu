@@ -30,6 +30,17 @@ static std::unordered_map<const void*, std::pair<int, unsigned>>& count_table() 
   static std::unordered_map<const void*, std::pair<int, unsigned>> t;
   return t;
 }
+// Device wait bound of the launches that use a workspace (set by
+// sinvb_rgf_batched_set_wait_limit; absent: kTeamWaitNs).
+static std::unordered_map<const void*, unsigned long long>& wait_table() {
+  static std::unordered_map<const void*, unsigned long long> t;
+  return t;
+}
+static unsigned long long wait_limit_of(const void* ws) {
+  std::lock_guard<std::mutex> lock(g_count_mutex);
+  auto it = wait_table().find(ws);
+  return it == wait_table().end() ? kTeamWaitNs : it->second;
+}
 
 template <class T>
 struct BatchEntry {
@@ -72,14 +83,16 @@ struct ItemArea {
   unsigned counter;  // team barrier arrivals
   int status;        // device status of the instance
   unsigned char* scratch;  // scratch slot of the team's rank-0 CTA
-  unsigned pad[12];
+  int slot_id;       // its index in the slot bitmap (-1: none)
+  unsigned left;     // members that have finished with the instance
+  unsigned pad[10];
 };
 static_assert(sizeof(ItemArea) == 64, "64-byte item areas");
 
 // Scratch slots are taken by a team's rank 0 from the bitmap hdr->slot_bits
 // (hdr->nslots slots, at least as many as teams that can run at once, so a
 // slot is normally free at once; the wait is bounded all the same).
-__device__ inline int acquire_scratch(WsHeader* hdr, int* status) {
+__device__ inline int acquire_scratch(WsHeader* hdr, int* status, unsigned long long wait_ns) {
   const int K = (int)hdr->nslots;
   unsigned long long t0 = 0;
   for (unsigned spins = 0;; spins++) {
@@ -99,7 +112,7 @@ __device__ inline int acquire_scratch(WsHeader* hdr, int* status) {
     if ((spins & 255) == 255) {
       const unsigned long long now = global_ns();
       if (t0 == 0) t0 = now;
-      else if (now - t0 > kTeamWaitNs) {
+      else if (now - t0 > wait_ns) {
         report(status, SINVB_STATUS_TIMEOUT);
         return -1;
       }
@@ -108,21 +121,22 @@ __device__ inline int acquire_scratch(WsHeader* hdr, int* status) {
 }
 // Streamed batches: the inputs of instance k are in place once ready[k]
 // holds this call's generation (written by a copy after the data, in stream
-// order); a bounded wait, reported as a timeout.
-__device__ inline void wait_ready(const WsHeader* hdr, int k, int* status) {
+// order); a bounded wait.  Returns false (timeout reported) when the word
+// never came; the instance is then skipped.
+__device__ inline bool wait_ready(const WsHeader* hdr, int k, int* status, unsigned long long wait_ns) {
   const unsigned gen = hdr->gen;
   unsigned long long t0 = 0;
   for (unsigned spins = 0;; spins++) {
     unsigned v;
     asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(hdr->ready + k) : "memory");
-    if (v == gen) return;
+    if (v == gen) return true;
     __nanosleep(512);
     if ((spins & 255) == 255) {
       const unsigned long long now = global_ns();
       if (t0 == 0) t0 = now;
-      else if (now - t0 > kTeamWaitNs) {
+      else if (now - t0 > wait_ns) {
         report(status, SINVB_STATUS_TIMEOUT);
-        return;
+        return false;
       }
     }
   }
@@ -140,14 +154,39 @@ __device__ inline void release_scratch(WsHeader* hdr, int id) {
   atomicAnd(&hdr->slot_bits[id >> 5], ~(1u << (id & 31)));
 }
 
+// Called by thread 0 of every member once its CTA is done with the instance
+// (after a __syncthreads), on every path out of it: the last member to leave
+// returns the scratch slot.  A failed pivot leaves every member running to the
+// sweep's final barrier, a wait that gave up lets members leave at different
+// times; either way the slot comes free only when no member can touch it.
+__device__ inline void leave_item(WsHeader* hdr, ItemArea* item, int team) {
+  __threadfence();
+  if (atomicAdd(&item->left, 1u) == (unsigned)team - 1) {
+    __threadfence();  // rank 0 wrote slot_id before it left
+    const int id = *((volatile int*)&item->slot_id);
+    release_scratch(hdr, id);
+  }
+}
+
+// Thread 0 of rank 0: the instance's status to the caller's array and the
+// call-wide word, and (streamed calls) its done word.
+__device__ inline void finish_item(WsHeader* hdr, ItemArea* item, int orig) {
+  const int st = *((volatile int*)&item->status);
+  if (hdr->inst_status) hdr->inst_status[orig] = st;
+  if (st) report(&hdr->status, st);
+  signal_done(hdr, orig);
+}
+
 // Persistent: every CTA repeatedly takes one queue slot.  Slot s belongs to the
 // instance k with slot_start[k] <= s < slot_start[k] + team[k], with rank
 // s - slot_start[k] in that instance's team.  Slots are handed out in order,
 // so a team completes as soon as its last member frees up; with teams sized
 // by block size (large blocks first) members mostly arrive together.  Every
 // CTA of the launch is resident (cooperative launch), so each team wait ends.
+// wait_ns bounds every wait of the launch (team barriers, scratch slots,
+// streamed ready words).
 template <class T, bool Mixed>
-__global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char* ws) {
+__global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char* ws, unsigned long long wait_ns) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* smem = reinterpret_cast<T*>(smem_raw);
   WsHeader* hdr = reinterpret_cast<WsHeader*>(ws);
@@ -179,22 +218,23 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
     const BatchEntry<T> e = entries[k];
     ItemArea* item = items + k;
     const int rank = s - e.slot_start;
-    __shared__ int sh_scratch;
     if (rank == 0 && threadIdx.x == 0) {
-      if (hdr->ready) wait_ready(hdr, e.orig, &item->status);
-      const int id = acquire_scratch(hdr, &item->status);
-      sh_scratch = id;
+      // an instance whose streamed inputs never arrived is skipped
+      const bool ready = !hdr->ready || wait_ready(hdr, e.orig, &item->status, wait_ns);
+      const int id = ready ? acquire_scratch(hdr, &item->status, wait_ns) : -1;
+      item->slot_id = id;
       item->scratch = id < 0 ? nullptr : ws + hdr->slots_offset + (size_t)id * hdr->slot_bytes;
       __threadfence();
     }
-    TeamDyn team{&item->counter, &item->status, rank, e.team, 0u};
-    if (!team.sync()) {  // formation: the rank-0 scratch pointer is visible after this
-      if (rank == 0 && threadIdx.x == 0) signal_done(hdr, e.orig);
-      continue;
-    }
-    unsigned char* slot = *((unsigned char* volatile*)&item->scratch);
-    if (!slot) {  // no scratch slot came free (reported); the whole team skips
-      if (rank == 0 && threadIdx.x == 0) signal_done(hdr, e.orig);
+    TeamDyn team{&item->counter, &item->status, rank, e.team, 0u, wait_ns};
+    // formation: the rank-0 scratch pointer is visible after this; without a
+    // slot (inputs never arrived, or none came free; reported) the team skips
+    unsigned char* slot = team.sync() ? *((unsigned char* volatile*)&item->scratch) : nullptr;
+    if (!slot) {
+      if (threadIdx.x == 0) {
+        if (rank == 0) finish_item(hdr, item, e.orig);
+        leave_item(hdr, item, e.team);
+      }
       continue;
     }
     const size_t bb = (size_t)e.b * e.b;
@@ -231,14 +271,9 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
     else
       rgf_sweep<T, 64, 64, Mixed>(team, p, smem);
     __syncthreads();
-    if (rank == 0 && threadIdx.x == 0) {
-      int st = *((volatile int*)&item->status);
-      if (hdr->inst_status) hdr->inst_status[e.orig] = st;
-      if (st) report(&hdr->status, st);
-      // the sweep ended on a team barrier, so no member touches the slot any
-      // more; after a failure members may still be running: keep it taken
-      if (!st) release_scratch(hdr, sh_scratch);
-      signal_done(hdr, e.orig);
+    if (threadIdx.x == 0) {
+      if (rank == 0) finish_item(hdr, item, e.orig);
+      leave_item(hdr, item, e.team);
     }
   }
   if (Mixed) oz_teardown(&oz_state);
@@ -344,7 +379,8 @@ static int launch_batched(void* ws, int count, unsigned flags, cudaStream_t stre
   const size_t items_offset = align_up(sizeof(WsHeader) + (size_t)count * sizeof(BatchEntry<cplx>), 256);
   SINVB_CUDA(cudaMemsetAsync((unsigned char*)ws + items_offset, 0, (size_t)count * sizeof(ItemArea), stream));
   unsigned char* w = (unsigned char*)ws;
-  void* args[] = {(void*)&w};
+  unsigned long long wait_ns = wait_limit_of(ws);
+  void* args[] = {(void*)&w, (void*)&wait_ns};
   // cooperative: every CTA resident, so a team member waiting for the others always gets them
   SINVB_CUDA(cudaLaunchCooperativeKernel((const void*)k, dim3(batch_slots()), dim3(kThreads), args, smem,
                                          stream));
@@ -469,6 +505,13 @@ int sinvb_rgf_batched_stream_d(const sinvb_batch_desc* descs, int count, unsigne
   if (flags & SINVB_PREC_MIXED) return SINVB_EUNSUPPORTED;
   return upload_and_run<double>(descs, count, flags, workspace, workspace_bytes, status, (cudaStream_t)stream,
                                 SINVB_F64, ready, done, gen);
+}
+
+int sinvb_rgf_batched_set_wait_limit(const void* workspace, double seconds) {
+  if (!workspace || !(seconds > 0.0) || seconds > 3600.0) return SINVB_EINVAL;
+  std::lock_guard<std::mutex> lock(g_count_mutex);
+  wait_table()[workspace] = (unsigned long long)(seconds * 1e9);
+  return SINVB_OK;
 }
 
 int sinvb_rgf_batched_rerun_z(void* workspace, sinvb_stream_t stream) {

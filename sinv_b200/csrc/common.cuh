@@ -148,6 +148,7 @@ struct TeamDyn {
   int* status;
   int r, n;
   unsigned generation;
+  unsigned long long wait_ns = kTeamWaitNs;  // bound of each wait (batched calls may lower it)
   __device__ int rank() const { return r; }
   __device__ int size() const { return n; }
   __device__ bool sync() {
@@ -172,7 +173,7 @@ struct TeamDyn {
           if ((spins & 1023) == 0) {
             unsigned long long now = global_ns();
             if (t0 == 0) t0 = now;
-            else if (now - t0 > kTeamWaitNs) {
+            else if (now - t0 > wait_ns) {
               report(status, SINVB_STATUS_TIMEOUT);
               good = 0;
               break;

@@ -1,10 +1,10 @@
 // Allocation-free RGF entry point.
 //
 // Some callers cannot allocate device memory at the point where they need a
-// selected inversion.  Examples: code running inside a CUDA stream capture
-// whose graph must not contain allocation nodes; a host callback or an
-// allocator hook that must not re-enter the allocator; a sandboxed plugin whose
-// host application owns every device allocation.  For them this file provides
+// selected inversion.  Examples: a host callback or an allocator hook that
+// must not re-enter the allocator; a sandboxed plugin whose host application
+// owns every device allocation and hands it only inputs and outputs.  For
+// them this file provides
 // sinvb_rgf_z_noalloc: the single-matrix RGF sweep (one CTA walks the whole
 // sweep) with its scratch memory in a file-scope device array that belongs to
 // the library, so the caller passes only the inputs and the outputs.
@@ -14,9 +14,13 @@
 //    (the sweep keeps its per-block-row products in G_upper / G_lower);
 //  * the array is kNoAllocScratchBytes (131,328 bytes); every GPU that loads
 //    the library holds it until the process exits;
-//  * the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current; make that first call
+//  * the first call on a device does the set-up with that device current: it
+//    looks up the array's device address (cudaGetSymbolAddress) and sets the
+//    shared-memory attribute of both kernel instances; make that first call
 //    before any stream capture;
+//  * the output arrays must not overlap the inputs or each other (the sweep
+//    keeps per-row products in G_upper / G_lower while it still reads A);
+//    overlapping ranges are rejected with SINVB_EINVAL;
 //  * every call uses the same array: calls that overlap on the GPU (two
 //    streams, or two threads) race on it and must be serialised by the caller;
 //  * the array keeps the contents of the last call; each call clears the
@@ -38,22 +42,6 @@ constexpr int kNoAllocDevices = 64;
 static void* g_noalloc_addr[kNoAllocDevices];
 static std::mutex g_noalloc_mutex;
 
-// Device address of g_noalloc_scratch on the current device (looked up once per device).
-static int noalloc_scratch(void** out) {
-  int dev = 0;
-  SINVB_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kNoAllocDevices) return SINVB_EUNSUPPORTED;
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    SINVB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    if (!p) return SINVB_ECUDA;
-    g_noalloc_addr[dev] = p;
-  }
-  *out = g_noalloc_addr[dev];
-  return SINVB_OK;
-}
-
 template <int BM, int BN>
 __global__ void __launch_bounds__(kThreads, 1) rgf_noalloc_kernel(RgfParams<cplx> p, int* status_out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -64,13 +52,44 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_noalloc_kernel(RgfParams<cplx
 }
 
 template <int BM, int BN>
-static int launch_noalloc(const RgfParams<cplx>& p, int* status_out, cudaStream_t stream) {
+constexpr size_t noalloc_smem() {
   constexpr size_t g = (size_t)gemm_smem_elems<cplx, BM, BN>() * sizeof(cplx);
-  constexpr size_t smem = g > sizeof(GjShared<cplx>) ? g : sizeof(GjShared<cplx>);
-  auto k = rgf_noalloc_kernel<BM, BN>;
-  SINVB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k<<<1, kThreads, smem, stream>>>(p, status_out);
+  return g > sizeof(GjShared<cplx>) ? g : sizeof(GjShared<cplx>);
+}
+
+template <int BM, int BN>
+static int launch_noalloc(const RgfParams<cplx>& p, int* status_out, cudaStream_t stream) {
+  rgf_noalloc_kernel<BM, BN><<<1, kThreads, noalloc_smem<BM, BN>(), stream>>>(p, status_out);
   SINVB_CUDA(cudaGetLastError());
+  return SINVB_OK;
+}
+
+// True when the byte ranges [a, a + na) and [b, b + nb) share a byte.
+static bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
+  if (!a || !b || !na || !nb) return false;
+  const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+  return x < y + nb && y < x + na;
+}
+
+// Device address of g_noalloc_scratch on the current device (looked up once per device).
+static int noalloc_scratch(void** out) {
+  int dev = 0;
+  SINVB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocDevices) return SINVB_EUNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    SINVB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    if (!p) return SINVB_ECUDA;
+    // both kernel instances get their shared-memory size now, so that no
+    // later call (whatever its b) performs device set-up
+    SINVB_CUDA(cudaFuncSetAttribute(rgf_noalloc_kernel<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)noalloc_smem<32, 32>()));
+    SINVB_CUDA(cudaFuncSetAttribute(rgf_noalloc_kernel<64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)noalloc_smem<64, 64>()));
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
   return SINVB_OK;
 }
 
@@ -89,6 +108,20 @@ extern "C" int sinvb_rgf_z_noalloc(const void* diag, const void* upper, const vo
   if (flags & ~(SINVB_SYM | SINVB_SAVE_OFFDIAG)) return SINVB_EINVAL;
   for (const void* q : {diag, upper, lower, (const void*)G_diag, (const void*)G_upper, (const void*)G_lower})
     if (q && (uintptr_t)q % 16) return SINVB_EINVAL;
+  {  // outputs may overlap neither the inputs nor each other
+    const size_t bb = (size_t)b * b * sizeof(cplx);
+    const size_t nd = (size_t)n * bb, no = n > 1 ? (size_t)(n - 1) * bb : 0;
+    const void* in[3] = {diag, upper, lower};
+    const size_t in_n[3] = {nd, no, no};
+    const void* out[3] = {G_diag, G_upper, G_lower};
+    const size_t out_n[3] = {nd, no, no};
+    for (int o = 0; o < 3; o++) {
+      for (int i = 0; i < 3; i++)
+        if (overlaps(out[o], out_n[o], in[i], in_n[i])) return SINVB_EINVAL;
+      for (int o2 = o + 1; o2 < 3; o2++)
+        if (overlaps(out[o], out_n[o], out[o2], out_n[o2])) return SINVB_EINVAL;
+    }
+  }
   int rc = check_device();
   if (rc) return rc;
   void* scratch = nullptr;

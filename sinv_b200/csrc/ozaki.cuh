@@ -659,7 +659,10 @@ __device__ inline void oz_slice_ops(int S, const GemmOp<cplx>* ops, const OzOp* 
 template <class Team>
 __device__ bool team_gemm_ozaki(Team& team, const GemmOp<cplx>* ops, int nops, int S, unsigned char* scratch,
                                 OzState* st, unsigned char* smem, int* status) {
-  if (st->fail) return false;
+  if (st->fail) {  // an earlier wait of this CTA gave up: its pipeline state is unknown
+    report(status, SINVB_STATUS_TIMEOUT);
+    return false;
+  }
   OzOp oz[2];
   unsigned char* p = scratch;
   for (int i = 0; i < nops; i++) {

@@ -178,3 +178,62 @@ def test_batch_rerun_captured_in_cuda_graph(precision):
     ref = rgf_batched([new], precision=precision)[0]
     for g, r in zip(plan.results()[0], ref):
         assert _rel(g.cpu().numpy(), r) <= 1e-12
+
+
+def test_failed_pivots_release_their_scratch_slots():
+    """More singular instances than scratch slots (one slot per concurrent
+    team: 148 on a B200 for b < 256), then healthy ones.  A failed pivot must
+    not keep its slot: every healthy instance gets one and finishes OK, with
+    no instance timing out.  The wait bound is lowered to 5 s so a regression
+    shows as SINVB_STATUS_TIMEOUT instead of minutes of waiting."""
+    from sinv_b200 import _lib
+    singular, healthy = 200, 40
+    inst = []
+    for k in range(singular + healthy):
+        d, u, l = workloads.dominant(3, 16, seed=900 + k)
+        if k < singular:
+            d = d.copy()
+            d[0] = 0.0  # the first block inverse meets a zero pivot
+        inst.append((d, u, l))
+    plan = BatchPlan(inst, wait_limit=5.0)
+    plan.run()
+    st = plan.statuses()
+    assert np.all(st[:singular] == _lib.STATUS_PIVOT), np.unique(st[:singular], return_counts=True)
+    assert np.all(st[singular:] == _lib.OK), np.unique(st[singular:], return_counts=True)
+    res = plan.results(like=inst[0][0])
+    for k in range(singular, singular + healthy, 7):
+        _check(res[k], rgf_oracle.rgf(*inst[k]), 1e-12)
+
+
+@pytest.mark.parametrize("shapes", [[(4, 32)] * 6, [(2, 64), (3, 256), (2, 64)]])
+def test_streamed_wait_runs_out_for_a_missing_instance(shapes):
+    """A streamed batch whose ready word for one instance is never written:
+    that instance's bounded wait (lowered to 50 ms) runs out, it reports
+    SINVB_STATUS_TIMEOUT and is skipped, the launch returns, and every other
+    instance is correct.  No fault, no trap: a device wait that gives up."""
+    import torch
+    from sinv_b200 import _lib
+    inst = [workloads.tight_binding(n, b, 0.3 + 0.1 * k, seed=950 + k) for k, (n, b) in enumerate(shapes)]
+    tinst = [tuple(torch.from_numpy(x).cuda() for x in t) for t in inst]
+    missing = len(inst) // 2
+    count = len(inst)
+    gen = 7
+    ready = torch.full((count,), gen, dtype=torch.int32, device="cuda")
+    ready[missing] = 0
+    done = torch.zeros(count, dtype=torch.int32, device="cuda")
+    plan = BatchPlan(tinst, wait_limit=0.05)
+    plan.run_streamed(ready, done, gen)
+    torch.cuda.synchronize()  # the launch ends although one instance never became ready
+    st = plan.statuses()
+    assert st[missing] == _lib.STATUS_TIMEOUT
+    assert all(st[k] == _lib.OK for k in range(count) if k != missing), st
+    assert torch.all(done == gen)  # the skipped instance is signalled done too
+    res = plan.results()
+    for k in range(count):
+        if k != missing:
+            _check([g.cpu().numpy() for g in res[k]], rgf_oracle.rgf(*inst[k]), 1e-11)
+    # the same plan, all inputs ready, default bound: every instance is OK again
+    plan.set_wait_limit(60.0)
+    ready.fill_(gen + 1)
+    plan.run_streamed(ready, done, gen + 1)
+    plan.check()

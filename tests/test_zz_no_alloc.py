@@ -1,9 +1,8 @@
 """The allocation-free entry point against the workspace-taking one.
 
 ``sinvb_rgf_z_noalloc`` serves callers that cannot allocate device memory at
-call time (inside a stream capture whose graph must hold no allocation nodes,
-inside an allocator hook or host callback, or in a plugin whose host owns all
-device memory).  Its scratch is a static device array inside the library, so
+call time (inside an allocator hook or host callback that must not re-enter
+the allocator, or in a plugin whose host owns all device memory).  Its scratch is a static device array inside the library, so
 this test passes only inputs and outputs, calls it twice in a row (the array
 keeps the previous call's contents, which must not leak into the next
 result), and compares both results with ``sinvb_rgf_z`` at the plain-path
@@ -108,3 +107,22 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     rc = lib.sinvb_rgf_z_noalloc(d.data_ptr(), u.data_ptr(), l.data_ptr(), 2, 64, 0, outs[0].data_ptr(),
                                  None, None, None, stream)
     assert rc == _lib.EINVAL
+
+
+def test_noalloc_rejects_outputs_that_overlap_inputs():
+    """The sweep keeps per-row products in G_upper / G_lower while it still
+    reads A, so an output array over an input (or over another output) would
+    give wrong results silently: the call refuses it."""
+    import torch
+    lib = _lib.load()
+    stream = torch.cuda.current_stream().cuda_stream
+    d, u, l = (_dev(x) for x in workloads.dominant(4, 16, seed=4))
+    Gd, Gu, Gl = (torch.empty_like(x) for x in (d, u, l))
+    for outs in [(d, Gu, Gl), (Gd, u, Gl), (Gd, Gu, l), (Gd, Gl, Gl), (Gd, Gu, u[1:])]:
+        rc = lib.sinvb_rgf_z_noalloc(d.data_ptr(), u.data_ptr(), l.data_ptr(), 4, 16, _lib.SAVE_OFFDIAG,
+                                     outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr(), None, stream)
+        assert rc == _lib.EINVAL
+    rc = lib.sinvb_rgf_z_noalloc(d.data_ptr(), u.data_ptr(), l.data_ptr(), 4, 16, _lib.SAVE_OFFDIAG,
+                                 Gd.data_ptr(), Gu.data_ptr(), Gl.data_ptr(), None, stream)
+    assert rc == _lib.OK
+    torch.cuda.synchronize()
