@@ -86,10 +86,16 @@ template <> struct GemmCfg<double> {
   template <int BN> __device__ static int b_idx(int k, int n) { return k * BN + (n ^ ((k & 3) << 2)); }
 };
 
-// Shared memory (in elements of T) one CTA tile needs.
+// Shared memory (in elements of T) one CTA tile needs: the K-chunk ring, then
+// the addend tile D (rows padded by one element against bank conflicts),
+// fetched with the first chunk so the epilogue does not wait on global loads.
+template <class T, int BM, int BN>
+__host__ __device__ constexpr int gemm_ring_elems() {
+  return kStages * (BM * GemmCfg<T>::BK + GemmCfg<T>::BK * BN);
+}
 template <class T, int BM, int BN>
 __host__ __device__ constexpr int gemm_smem_elems() {
-  return kStages * (BM * GemmCfg<T>::BK + GemmCfg<T>::BK * BN);
+  return gemm_ring_elems<T, BM, BN>() + BM * (BN + 1);
 }
 
 // K extent of the first product as streamed: padded to whole chunks when a
@@ -207,11 +213,16 @@ __device__ __forceinline__ void mma_chunk(const double* sA, const double* sB, do
   }
 }
 
+// Epilogue of two adjacent outputs (r, c), (r, c+1): alpha times the
+// accumulators plus beta times the addend, whose tile sits in shared memory
+// at dtile (row stride ldt, indexed from the tile origin; null: no addend).
 template <class T>
-__device__ __forceinline__ void store_pair(const GemmOp<T>& op, int r, int c, double v0r, double v0i, double v1r, double v1i);
+__device__ __forceinline__ void store_pair(const GemmOp<T>& op, int r, int c, const T* dtile, int ldt, double v0r,
+                                           double v0i, double v1r, double v1i);
 
 template <>
-__device__ __forceinline__ void store_pair<cplx>(const GemmOp<cplx>& op, int r, int c, double v0r, double v0i, double v1r, double v1i) {
+__device__ __forceinline__ void store_pair<cplx>(const GemmOp<cplx>& op, int r, int c, const cplx* dtile, int ldt,
+                                                 double v0r, double v0i, double v1r, double v1i) {
   if (r >= op.M) return;
   const double al = op.alpha, be = op.beta;
 #pragma unroll
@@ -219,8 +230,8 @@ __device__ __forceinline__ void store_pair<cplx>(const GemmOp<cplx>& op, int r, 
     int cc = c + j;
     if (cc < op.N) {
       cplx v = j == 0 ? cplx{al * v0r, al * v0i} : cplx{al * v1r, al * v1i};
-      if (op.D) {
-        cplx d = op.D[(size_t)r * op.ldd + cc];
+      if (dtile) {
+        cplx d = dtile[j];
         v = be == 1.0 ? d + v : cplx{fma(be, d.re, v.re), fma(be, d.im, v.im)};
       }
       op.C[(size_t)r * op.ldc + cc] = v;
@@ -228,18 +239,33 @@ __device__ __forceinline__ void store_pair<cplx>(const GemmOp<cplx>& op, int r, 
   }
 }
 template <>
-__device__ __forceinline__ void store_pair<double>(const GemmOp<double>& op, int r, int c, double v0, double, double v1, double) {
+__device__ __forceinline__ void store_pair<double>(const GemmOp<double>& op, int r, int c, const double* dtile, int ldt,
+                                                   double v0, double, double v1, double) {
   if (r >= op.M) return;
   const double al = op.alpha, be = op.beta;
   if (c < op.N) {
     double v = al * v0;
-    if (op.D) v = fma(be, op.D[(size_t)r * op.ldd + c], v);
+    if (dtile) v = fma(be, dtile[0], v);
     op.C[(size_t)r * op.ldc + c] = v;
   }
   if (c + 1 < op.N) {
     double v = al * v1;
-    if (op.D) v = fma(be, op.D[(size_t)r * op.ldd + c + 1], v);
+    if (dtile) v = fma(be, dtile[1], v);
     op.C[(size_t)r * op.ldc + c + 1] = v;
+  }
+}
+
+// Asynchronous copy of the addend tile D[row0 .., col0 ..] (the part inside
+// M x N) into shared memory, row stride BN + 1; consecutive threads take
+// consecutive columns.
+template <class T, int BM, int BN>
+__device__ __forceinline__ void load_addend(const GemmOp<T>& op, int row0, int col0, T* sD) {
+#pragma unroll 4
+  for (int e = threadIdx.x; e < BM * BN; e += kThreads) {
+    const int r = e / BN, c = e % BN;
+    const bool v = row0 + r < op.M && col0 + c < op.N;
+    const T* src = v ? op.D + (size_t)(row0 + r) * op.ldd + (col0 + c) : op.D;
+    cp_async_elem<T>(sD + r * (BN + 1) + c, src, v);
   }
 }
 
@@ -268,6 +294,9 @@ __device__ void cta_gemm_tile(const GemmOp<T>& op, int tm, int tn, T* smem) {
   const double sai1 = op.opA == kOpH ? -1.0 : 1.0, sbi1 = op.opB == kOpH ? -1.0 : 1.0;
   const double s2 = op.sign2 < 0 ? -1.0 : 1.0;
   const double sai2 = op.opA2 == kOpH ? -1.0 : 1.0, sbi2 = (op.opB2 == kOpH ? -1.0 : 1.0) * s2;
+  T* sD = smem + gemm_ring_elems<T, BM, BN>();
+  const bool addend = op.D != nullptr;
+  if (addend) load_addend<T, BM, BN>(op, row0, col0, sD);  // lands with the first chunk's group
 #pragma unroll
   for (int s = 0; s < kStages - 1; s++) {
     if (s < nk) load_chunk<T, BM, BN>(op, row0, col0, s * BK, sA + s * BM * BK, sB + s * BK * BN);
@@ -289,6 +318,7 @@ __device__ void cta_gemm_tile(const GemmOp<T>& op, int tm, int tn, T* smem) {
       mma_chunk<BM, BN>(sA + st * BM * BK, sB + st * BK * BN, acc, sai2, s2, sbi2);
   }
   cp_async_wait<0>();
+  __syncthreads();  // the addend tile, copied by every thread, is complete
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
@@ -297,9 +327,9 @@ __device__ void cta_gemm_tile(const GemmOp<T>& op, int tm, int tn, T* smem) {
   for (int mt = 0; mt < W::MT; mt++)
 #pragma unroll
     for (int nt = 0; nt < W::NT; nt++) {
-      int r = row0 + wm + mt * 8 + g;
-      int c = col0 + wn + nt * 8 + 2 * t;
-      store_pair<T>(op, r, c, acc[mt][nt][0], acc[mt][nt][2], acc[mt][nt][1], acc[mt][nt][3]);
+      const int lr = wm + mt * 8 + g, lc = wn + nt * 8 + 2 * t;
+      store_pair<T>(op, row0 + lr, col0 + lc, addend ? sD + lr * (BN + 1) + lc : nullptr, BN + 1, acc[mt][nt][0],
+                    acc[mt][nt][2], acc[mt][nt][1], acc[mt][nt][3]);
     }
   __syncthreads();
 }

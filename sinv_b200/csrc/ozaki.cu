@@ -15,11 +15,10 @@ static size_t oz_workspace_bytes(int M, int N, int K, int S) { return sizeof(WsH
 // others 32-column blocks of B.
 __global__ void __launch_bounds__(256) oz_slice_kernel(GemmOp<cplx> g, OzOp op, int ctas_a) {
   extern __shared__ __align__(16) unsigned char slice_smem[];
-  const int never = 1 << 30;
   if ((int)blockIdx.x < ctas_a)
-    oz_slice_ops(op.s.S, &g, &op, 1, blockIdx.x, ctas_a, never, 1, slice_smem);
+    oz_slice_ops(op.s.S, &g, &op, 1, 1u, 0u, blockIdx.x, ctas_a, 0, 1, slice_smem);
   else
-    oz_slice_ops(op.s.S, &g, &op, 1, never, 1, blockIdx.x - ctas_a, gridDim.x - ctas_a, slice_smem);
+    oz_slice_ops(op.s.S, &g, &op, 1, 0u, 1u, 0, 1, blockIdx.x - ctas_a, gridDim.x - ctas_a, slice_smem);
 }
 
 // Persistent over output tiles: every CTA allocates TMEM once and walks tiles

@@ -625,29 +625,53 @@ __host__ __device__ constexpr size_t oz_slice_smem(int S) {
   return oz_slice_a_smem(S) > 4 * 256 * 8 + 4 * 32 * 8 ? oz_slice_a_smem(S) : 4 * 256 * 8 + 4 * 32 * 8;
 }
 
+// Operands to slice: bit i of slice_a / slice_b for op i's A / B (an operand
+// whose planes are already in place, from an earlier call or another op of
+// this one, is skipped).
 template <int S>
-__device__ inline void oz_slice_ops_s(const GemmOp<cplx>* ops, const OzOp* oz, int nops, int a0, int astep, int b0,
-                                      int bstep, unsigned char* smem) {
+__device__ inline void oz_slice_ops_s(const GemmOp<cplx>* ops, const OzOp* oz, int nops, unsigned slice_a,
+                                      unsigned slice_b, int a0, int astep, int b0, int bstep, unsigned char* smem) {
   for (int i = 0; i < nops; i++) {
-    oz_slice_a<S>(ops[i].A, ops[i].lda, oz[i].s, const_cast<int8_t*>(oz[i].a_planes), const_cast<int*>(oz[i].ea), a0,
-                  astep, smem);
-    oz_slice_b<S>(ops[i].B, ops[i].ldb, oz[i].s, const_cast<int8_t*>(oz[i].b_planes), const_cast<int*>(oz[i].fb), b0,
-                  bstep, reinterpret_cast<double*>(smem));
+    if ((slice_a >> i) & 1u)
+      oz_slice_a<S>(ops[i].A, ops[i].lda, oz[i].s, const_cast<int8_t*>(oz[i].a_planes), const_cast<int*>(oz[i].ea),
+                    a0, astep, smem);
+    if ((slice_b >> i) & 1u)
+      oz_slice_b<S>(ops[i].B, ops[i].ldb, oz[i].s, const_cast<int8_t*>(oz[i].b_planes), const_cast<int*>(oz[i].fb),
+                    b0, bstep, reinterpret_cast<double*>(smem));
   }
 }
 
-__device__ inline void oz_slice_ops(int S, const GemmOp<cplx>* ops, const OzOp* oz, int nops, int a0, int astep,
-                                    int b0, int bstep, unsigned char* smem) {
+__device__ inline void oz_slice_ops(int S, const GemmOp<cplx>* ops, const OzOp* oz, int nops, unsigned slice_a,
+                                    unsigned slice_b, int a0, int astep, int b0, int bstep, unsigned char* smem) {
   switch (S) {
-    case 1: oz_slice_ops_s<1>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
-    case 2: oz_slice_ops_s<2>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
-    case 3: oz_slice_ops_s<3>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
-    case 4: oz_slice_ops_s<4>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
-    case 5: oz_slice_ops_s<5>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
-    case 6: oz_slice_ops_s<6>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
-    case 7: oz_slice_ops_s<7>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
-    default: oz_slice_ops_s<8>(ops, oz, nops, a0, astep, b0, bstep, smem); break;
+    case 1: oz_slice_ops_s<1>(ops, oz, nops, slice_a, slice_b, a0, astep, b0, bstep, smem); break;
+    case 2: oz_slice_ops_s<2>(ops, oz, nops, slice_a, slice_b, a0, astep, b0, bstep, smem); break;
+    case 3: oz_slice_ops_s<3>(ops, oz, nops, slice_a, slice_b, a0, astep, b0, bstep, smem); break;
+    case 4: oz_slice_ops_s<4>(ops, oz, nops, slice_a, slice_b, a0, astep, b0, bstep, smem); break;
+    case 5: oz_slice_ops_s<5>(ops, oz, nops, slice_a, slice_b, a0, astep, b0, bstep, smem); break;
+    case 6: oz_slice_ops_s<6>(ops, oz, nops, slice_a, slice_b, a0, astep, b0, bstep, smem); break;
+    case 7: oz_slice_ops_s<7>(ops, oz, nops, slice_a, slice_b, a0, astep, b0, bstep, smem); break;
+    default: oz_slice_ops_s<8>(ops, oz, nops, slice_a, slice_b, a0, astep, b0, bstep, smem); break;
   }
+}
+
+// Operand slots of the team products: scratch holds two A-role slots (row
+// exponents and embedded digit planes) and two B-role slots (column exponents
+// and digit planes), each for an M x K (K x N) operand; 2 oz_op_scratch(M, N,
+// K, S) bytes in all.  A product names the slot of each operand and whether
+// the operand is sliced in this call or its planes are reused, so an operand
+// shared by consecutive products is sliced once.
+struct OzSlots {
+  int a[2], b[2];      // slot of op i's A / B operand
+  unsigned slice_a;    // bit i: slice op i's A into its slot
+  unsigned slice_b;    // bit i: slice op i's B into its slot
+};
+
+__host__ __device__ inline size_t oz_slot_a_bytes(const OzShape& s) {
+  return (size_t)oz_pad(s.M * 4, 256) + (size_t)s.S * s.a_plane();
+}
+__host__ __device__ inline size_t oz_slot_b_bytes(const OzShape& s) {
+  return (size_t)oz_pad(s.N * 4, 256) + (size_t)s.S * s.b_plane();
 }
 
 // Up to 2 independent complex block products C = beta D + alpha A B on the
@@ -656,20 +680,40 @@ __device__ inline void oz_slice_ops(int S, const GemmOp<cplx>* ops, const OzOp* 
 // and B column blocks over the CTAs of the team), then the output tiles
 // (over its CTAs).  The caller synchronises after the second.  Plain
 // (non-transposed) operands only.  Returns false when a wait gave up.
+//
+// The operands of all products of one sweep have the same shape (M = N = K =
+// the block size), so one slot size fits every operand; `slots` says which
+// operands this call slices and which planes it reuses (OzSlots).
 template <class Team>
 __device__ bool team_gemm_ozaki(Team& team, const GemmOp<cplx>* ops, int nops, int S, unsigned char* scratch,
-                                OzState* st, unsigned char* smem, int* status) {
+                                const OzSlots& slots, OzState* st, unsigned char* smem, int* status) {
   if (st->fail) {  // an earlier wait of this CTA gave up: its pipeline state is unknown
     report(status, SINVB_STATUS_TIMEOUT);
     return false;
   }
   OzOp oz[2];
-  unsigned char* p = scratch;
+  const OzShape s0 = oz_shape(ops[0].M, ops[0].N, ops[0].K, S);
+  const size_t sa = oz_slot_a_bytes(s0), sb = oz_slot_b_bytes(s0);
   for (int i = 0; i < nops; i++) {
     const GemmOp<cplx>& g = ops[i];
-    p = oz_bind(oz[i], g.M, g.N, g.K, S, p, g.alpha, g.beta, g.D, g.ldd, g.C, g.ldc);
+    OzOp& o = oz[i];
+    o.s = oz_shape(g.M, g.N, g.K, S);
+    o.tiles = oz_tile_count(o.s);
+    unsigned char* pa = scratch + (size_t)slots.a[i] * sa;
+    unsigned char* pb = scratch + 2 * sa + (size_t)slots.b[i] * sb;
+    o.ea = reinterpret_cast<int*>(pa);
+    o.a_planes = reinterpret_cast<int8_t*>(pa + oz_pad(g.M * 4, 256));
+    o.fb = reinterpret_cast<int*>(pb);
+    o.b_planes = reinterpret_cast<int8_t*>(pb + oz_pad(g.N * 4, 256));
+    o.D = g.D;
+    o.C = g.C;
+    o.ldd = g.ldd;
+    o.ldc = g.ldc;
+    o.alpha = g.alpha;
+    o.beta = g.beta;
   }
-  oz_slice_ops(S, ops, oz, nops, team.rank(), team.size(), team.rank(), team.size(), smem);
+  oz_slice_ops(S, ops, oz, nops, slots.slice_a, slots.slice_b, team.rank(), team.size(), team.rank(), team.size(),
+               smem);
   // the planes are read by the bulk-copy (async) proxy of every CTA of the team
   asm volatile("fence.proxy.async.global;" ::: "memory");
   if (!team.sync()) return false;

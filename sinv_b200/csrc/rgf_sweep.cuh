@@ -66,13 +66,18 @@ struct RgfParams {
 // The block products of a sweep phase: FP64 DMMA, or (Mixed, complex only)
 // the int8 tensor-core Ozaki products when p.oz_digits > 0.  The block
 // inverses always stay in FP64.  Mixed is a template switch so that kernels
-// without the tensor-core path do not carry its registers.
+// without the tensor-core path do not carry its registers.  `slots` places
+// the digit planes of the operands (two A and two B slots) so that an
+// operand shared by consecutive products is sliced once per phase:
+//   F1  g U (A0, B0), L g (A1, B1)     F2  P U (A1 sliced, B0 = U reused)
+//   B1  G P (A0, B0)                   B2  X G (A1, B1), X T (A1 = X reused, B0)
 template <class T, int BM, int BN, bool Mixed, class Team>
-__device__ __forceinline__ bool sweep_gemm(Team& team, const RgfParams<T>& p, const GemmOp<T>* ops, int nops, T* smem) {
+__device__ __forceinline__ bool sweep_gemm(Team& team, const RgfParams<T>& p, const GemmOp<T>* ops, int nops, T* smem,
+                                           const OzSlots& slots) {
   if constexpr (Mixed && std::is_same<T, cplx>::value) {
     if (p.oz_digits > 0)
-      return team_gemm_ozaki(team, ops, nops, p.oz_digits, p.oz_scratch, p.oz, reinterpret_cast<unsigned char*>(smem),
-                             p.status);
+      return team_gemm_ozaki(team, ops, nops, p.oz_digits, p.oz_scratch, slots, p.oz,
+                             reinterpret_cast<unsigned char*>(smem), p.status);
   }
   team_gemm<T, BM, BN>(team, ops, nops, smem);
   return true;
@@ -105,7 +110,7 @@ __device__ void rgf_sweep(Team& team, const RgfParams<T>& p, T* smem) {
       GemmOp<T> ops[2];
       ops[0] = make_op<T>(b, b, b, 1.0, g, b, U, b, nullptr, 0, Xd, b);
       ops[1] = make_op<T>(b, b, b, 1.0, L, b, g, b, nullptr, 0, Pd, b);
-      if (!sweep_gemm<T, BM, BN, Mixed>(team, p, ops, 2, smem)) return;
+      if (!sweep_gemm<T, BM, BN, Mixed>(team, p, ops, 2, smem, OzSlots{{0, 1}, {0, 1}, 3u, 3u})) return;
       if (inplace && i >= 2)  // P_{i-1} over A_{i-2,i-1}, dead since F2 of step i-1
         team_copy<T>(team, b, b, (i & 1) ? p.T1 : p.T3, b, p.Gu + (i - 2) * bb, b);
       if (p.ckpt && i % p.ckpt_every == 0)  // checkpoint g_{i-1} for the adjoint
@@ -114,7 +119,7 @@ __device__ void rgf_sweep(Team& team, const RgfParams<T>& p, T* smem) {
     if (!team.sync()) return;
     {  // F2: S_i = A_ii - P_i U_{i-1}
       GemmOp<T> op = make_op<T>(b, b, b, -1.0, Pd, b, U, b, p.diag + i * bb, b, p.Gd + i * bb, b);
-      if (!sweep_gemm<T, BM, BN, Mixed>(team, p, &op, 1, smem)) return;
+      if (!sweep_gemm<T, BM, BN, Mixed>(team, p, &op, 1, smem, OzSlots{{1, 0}, {0, 0}, 1u, 0u})) return;
       if (inplace)  // X_{i-1} over A_{i,i-1}, dead since F1
         team_copy<T>(team, b, b, Xd, b, p.Gl + (i - 1) * bb, b);
     }
@@ -132,7 +137,7 @@ __device__ void rgf_sweep(Team& team, const RgfParams<T>& p, T* smem) {
     T* Tcur = (i & 1) ? p.T1 : p.T0;
     {  // B1: T = -G_{i+1} P_{i+1}; flush the previous T into G_lower / G_upper
       GemmOp<T> op = make_op<T>(b, b, b, -1.0, p.Gd + (i + 1) * bb, b, p.P + i * bb, b, nullptr, 0, Tcur, b);
-      if (!sweep_gemm<T, BM, BN, Mixed>(team, p, &op, 1, smem)) return;
+      if (!sweep_gemm<T, BM, BN, Mixed>(team, p, &op, 1, smem, OzSlots{{0, 0}, {0, 0}, 1u, 1u})) return;
       if (prevT && save) {
         team_copy<T>(team, b, b, prevT, b, p.Gl + prevI * bb, b);
         if (sym) team_copy<T>(team, b, b, prevT, b, p.Gu + prevI * bb, b, true);
@@ -147,7 +152,9 @@ __device__ void rgf_sweep(Team& team, const RgfParams<T>& p, T* smem) {
         ops[q++] = make_op<T>(b, b, b, -1.0, X, b, p.Gd + (i + 1) * bb, b, nullptr, 0, p.Gu + i * bb, b);
       T* Gii = p.Gd + i * bb;
       ops[q++] = make_op<T>(b, b, b, -1.0, X, b, Tcur, b, Gii, b, Gii, b);
-      if (!sweep_gemm<T, BM, BN, Mixed>(team, p, ops, q, smem)) return;
+      // X is sliced once: by the first product, reused by the second
+      const OzSlots sl = q == 2 ? OzSlots{{1, 1}, {1, 0}, 1u, 3u} : OzSlots{{1, 0}, {0, 0}, 1u, 1u};
+      if (!sweep_gemm<T, BM, BN, Mixed>(team, p, ops, q, smem, sl)) return;
     }
     if (!team.sync()) return;
     prevT = Tcur;
