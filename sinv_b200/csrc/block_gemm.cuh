@@ -213,6 +213,52 @@ __device__ __forceinline__ void mma_chunk(const double* sA, const double* sB, do
   }
 }
 
+// The common product (no conjugation, no second product): no sign factors
+// on the fragments; -Im B by flipping its sign bit on the integer pipe.
+__device__ __forceinline__ double neg_bits(double x) {
+  return __hiloint2double(__double2hiint(x) ^ 0x80000000, __double2loint(x));
+}
+template <int BM, int BN>
+__device__ __forceinline__ void mma_chunk_plain(const cplx* sA, const cplx* sB,
+                                                double (&acc)[WarpShape<BM, BN>::MT][WarpShape<BM, BN>::NT][4]) {
+  using W = WarpShape<BM, BN>;
+  constexpr int BK = GemmCfg<cplx>::BK;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp >> 2) * W::WM, wn = (warp & 3) * W::WN;
+#pragma unroll
+  for (int kk = 0; kk < BK; kk += 4) {
+    cplx a[W::MT], b[W::NT];
+    double nbi[W::NT];
+#pragma unroll
+    for (int mt = 0; mt < W::MT; mt++) a[mt] = sA[GemmCfg<cplx>::a_idx(wm + mt * 8 + g, kk + t)];
+#pragma unroll
+    for (int nt = 0; nt < W::NT; nt++) {
+      b[nt] = sB[GemmCfg<cplx>::b_idx<BN>(kk + t, wn + nt * 8 + g)];
+      nbi[nt] = neg_bits(b[nt].im);
+    }
+#pragma unroll
+    for (int mt = 0; mt < W::MT; mt++)
+#pragma unroll
+      for (int nt = 0; nt < W::NT; nt++) {
+        dmma884(acc[mt][nt][0], acc[mt][nt][1], a[mt].re, b[nt].re);
+        dmma884(acc[mt][nt][2], acc[mt][nt][3], a[mt].re, b[nt].im);
+      }
+#pragma unroll
+    for (int mt = 0; mt < W::MT; mt++)
+#pragma unroll
+      for (int nt = 0; nt < W::NT; nt++) {
+        dmma884(acc[mt][nt][0], acc[mt][nt][1], a[mt].im, nbi[nt]);
+        dmma884(acc[mt][nt][2], acc[mt][nt][3], a[mt].im, b[nt].re);
+      }
+  }
+}
+template <int BM, int BN>
+__device__ __forceinline__ void mma_chunk_plain(const double* sA, const double* sB,
+                                                double (&acc)[WarpShape<BM, BN>::MT][WarpShape<BM, BN>::NT][4]) {
+  mma_chunk<BM, BN>(sA, sB, acc, 1.0, 1.0, 1.0);
+}
+
 // Epilogue of two adjacent outputs (r, c), (r, c+1): alpha times the
 // accumulators plus beta times the addend, whose tile sits in shared memory
 // at dtile (row stride ldt, indexed from the tile origin; null: no addend).
@@ -269,8 +315,19 @@ __device__ __forceinline__ void load_addend(const GemmOp<T>& op, int row0, int c
   }
 }
 
-// One output tile (tile row tm, tile column tn) of op, computed by the whole CTA.
-// smem: gemm_smem_elems<T,BM,BN>() elements.  Ends with the CTA synchronised and
+template <class T, int BM, int BN>
+__device__ __forceinline__ int op_tiles(const GemmOp<T>& op) {
+  if (op.M <= 0 || op.N <= 0) return 0;
+  return ((op.M + BM - 1) / BM) * ((op.N + BN - 1) / BN);
+}
+
+// One output tile (tile row tm, tile column tn) of op, computed by the whole
+// CTA.  K streams through a 3-stage cp.async ring; each chunk's successor
+// load is issued after the chunk's multiplications so that the DMMAs start
+// right after the barrier.  The addend tile D is fetched into shared memory
+// with the first chunk, so the epilogue does not wait on global loads (D may
+// alias C: the tile reads its own D before it writes C).  smem:
+// gemm_smem_elems<T,BM,BN>() elements.  Ends with the CTA synchronised and
 // the tile written.
 template <class T, int BM, int BN>
 __device__ void cta_gemm_tile(const GemmOp<T>& op, int tm, int tn, T* smem) {
@@ -278,6 +335,7 @@ __device__ void cta_gemm_tile(const GemmOp<T>& op, int tm, int tn, T* smem) {
   constexpr int BK = GemmCfg<T>::BK;
   T* sA = smem;
   T* sB = smem + kStages * BM * BK;
+  T* sD = smem + gemm_ring_elems<T, BM, BN>();
   const int row0 = tm * BM, col0 = tn * BN;
   double acc[W::MT][W::NT][4];
 #pragma unroll
@@ -290,11 +348,11 @@ __device__ void cta_gemm_tile(const GemmOp<T>& op, int tm, int tn, T* smem) {
   const int K1p = k1_padded(op);
   const int nk = (K1p + op.K2 + BK - 1) / BK;
   const int nk1 = (K1p + BK - 1) / BK;  // chunks of the first product
+  const bool plain = op.opA == kOpN && op.opB == kOpN;
   // fragment signs per product: conjugation of A / B, sign of the second product
   const double sai1 = op.opA == kOpH ? -1.0 : 1.0, sbi1 = op.opB == kOpH ? -1.0 : 1.0;
   const double s2 = op.sign2 < 0 ? -1.0 : 1.0;
   const double sai2 = op.opA2 == kOpH ? -1.0 : 1.0, sbi2 = (op.opB2 == kOpH ? -1.0 : 1.0) * s2;
-  T* sD = smem + gemm_ring_elems<T, BM, BN>();
   const bool addend = op.D != nullptr;
   if (addend) load_addend<T, BM, BN>(op, row0, col0, sD);  // lands with the first chunk's group
 #pragma unroll
@@ -305,17 +363,22 @@ __device__ void cta_gemm_tile(const GemmOp<T>& op, int tm, int tn, T* smem) {
   for (int kc = 0; kc < nk; kc++) {
     cp_async_wait<kStages - 2>();
     __syncthreads();
-    int pf = kc + kStages - 1;
+    const int st = kc % kStages;
+    if (kc < nk1) {
+      if (plain)
+        mma_chunk_plain<BM, BN>(sA + st * BM * BK, sB + st * BK * BN, acc);
+      else
+        mma_chunk<BM, BN>(sA + st * BM * BK, sB + st * BK * BN, acc, sai1, 1.0, sbi1);
+    } else {
+      mma_chunk<BM, BN>(sA + st * BM * BK, sB + st * BK * BN, acc, sai2, s2, sbi2);
+    }
+    // into the stage consumed one chunk ago: every warp is past this chunk's barrier
+    const int pf = kc + kStages - 1;
     if (pf < nk) {
-      int st = pf % kStages;
-      load_chunk<T, BM, BN>(op, row0, col0, pf * BK, sA + st * BM * BK, sB + st * BK * BN);
+      const int sp = pf % kStages;
+      load_chunk<T, BM, BN>(op, row0, col0, pf * BK, sA + sp * BM * BK, sB + sp * BK * BN);
     }
     cp_async_commit();
-    int st = kc % kStages;
-    if (kc < nk1)
-      mma_chunk<BM, BN>(sA + st * BM * BK, sB + st * BK * BN, acc, sai1, 1.0, sbi1);
-    else
-      mma_chunk<BM, BN>(sA + st * BM * BK, sB + st * BK * BN, acc, sai2, s2, sbi2);
   }
   cp_async_wait<0>();
   __syncthreads();  // the addend tile, copied by every thread, is complete
@@ -332,12 +395,6 @@ __device__ void cta_gemm_tile(const GemmOp<T>& op, int tm, int tn, T* smem) {
                     acc[mt][nt][2], acc[mt][nt][1], acc[mt][nt][3]);
     }
   __syncthreads();
-}
-
-template <class T, int BM, int BN>
-__device__ __forceinline__ int op_tiles(const GemmOp<T>& op) {
-  if (op.M <= 0 || op.N <= 0) return 0;
-  return ((op.M + BM - 1) / BM) * ((op.N + BN - 1) / BN);
 }
 
 // All tiles of up to 8 independent GEMMs, spread over the team's CTAs.  The
