@@ -197,63 +197,159 @@ def dmma_peak_tflops(torch):
     return best
 
 
-def cpu_sample(spec):
-    """Stratified CPU sample: the first instance of each block size."""
-    seen, idx = set(), []
+# The CPU baseline's fixed sample: the first PER_B instances of each block
+# size in the batch's order (same seeds and energies as the GPU run).
+PER_B = 2
+
+
+def cpu_sample(spec, per_b=PER_B):
+    """Stratified fixed sample of the batch: the first ``per_b`` instances of
+    each block size, in batch order."""
+    seen, idx = {}, []
     for k, (_, _, b, _) in enumerate(spec):
-        if b not in seen:
-            seen.add(b)
+        if seen.get(b, 0) < per_b:
+            seen[b] = seen.get(b, 0) + 1
             idx.append(k)
     return idx
 
 
-def cpu_baseline(spec, reps=1):
-    """The reference RGF (numpy restatement of src/sinv/algorithms/rgf/rgf.py) on host
-    cores, on one instance per block size; extrapolated to the whole batch by the
-    canonical flop count per block-size class."""
+def _cpu_env():
+    """Host threads the BLAS uses, and the host's core count."""
+    return {"blas_threads": _blas_threads(), "nproc": os.cpu_count() or 1,
+            "OPENBLAS_NUM_THREADS": os.environ.get("OPENBLAS_NUM_THREADS", "unset")}
+
+
+def _extrapolate(spec, spf_by_b):
+    """Seconds for the whole batch from seconds-per-canonical-flop per block size."""
+    from sinv_b200 import workloads
+    return sum(workloads.rgf_flops(n, b) * spf_by_b[b] for (_, n, b, _) in spec)
+
+
+def cpu_baseline(spec, reps=3):
+    """The reference RGF (numpy restatement of src/sinv/algorithms/rgf/rgf.py,
+    the same numpy / OpenBLAS calls in the same order) on the host cores: the
+    fixed stratified sample (two instances per block size), each timed
+    ``reps`` times after one untimed warm-up, median per instance; the batch
+    time is extrapolated from the median seconds per canonical flop of each
+    block size (marked as extrapolated)."""
     from oracle import rgf_oracle
     from sinv_b200 import workloads
-    try:
-        from threadpoolctl import threadpool_info
-        cores = max([i.get("num_threads", 1) for i in threadpool_info() if i.get("user_api") == "blas"] or [1])
-    except Exception:
-        cores = os.cpu_count() or 1
-    spf, sampled = {}, []
-    t_total = 0.0
-    for k in cpu_sample(spec):
+    idx = cpu_sample(spec)
+    spf = {}
+    timed, sampled = 0.0, []
+    warm = workloads.tight_binding(*spec[idx[0]][1:3], spec[idx[0]][0], seed=spec[idx[0]][3])
+    rgf_oracle.rgf(*warm)
+    for k in idx:
         e, n, b, s = spec[k]
         d, u, l = workloads.tight_binding(n, b, e, seed=s)
-        best = 1e30
+        ts = []
         for _ in range(reps):
             t0 = time.perf_counter()
             rgf_oracle.rgf(d, u, l)
-            best = min(best, time.perf_counter() - t0)
-        t_total += best
-        spf[b] = best / workloads.rgf_flops(n, b)
-        sampled.append("n=%d,b=%d:%.2fs" % (n, b, best))
-    t_batch = sum(workloads.rgf_flops(n, b) * spf[b] for (_, n, b, _) in spec)
-    return {"value": len(spec) / t_batch, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": "reference rgf (numpy/OpenBLAS restatement) on one instance per block size [%s], "
-                      "extrapolated to the %d-instance batch by the canonical flop count per block size"
-                      % (", ".join(sampled), len(spec)),
-            "sample_seconds": t_total}
+            ts.append(time.perf_counter() - t0)
+        timed += sum(ts)
+        med = statistics.median(ts)
+        spf.setdefault(b, []).append(med / workloads.rgf_flops(n, b))
+        sampled.append("n=%d,b=%d:%.3fs" % (n, b, med))
+    spf_med = {b: statistics.median(v) for b, v in spf.items()}
+    t_batch = _extrapolate(spec, spf_med)
+    env = _cpu_env()
+    return {"value": len(spec) / t_batch, "unit": UNIT, "cores": env["blas_threads"], "kind": "port",
+            "sample": "reference rgf (numpy/OpenBLAS restatement) on a fixed stratified sample (the first %d "
+                      "instances of each block size: %s), median of %d timed runs each after a warm-up; "
+                      "batch time extrapolated from the median seconds per canonical flop of each block size"
+                      % (PER_B, ", ".join(sampled), reps),
+            "extrapolated": True, "timed_seconds": timed,
+            "spread_seconds_per_flop": {str(b): [min(v), max(v)] for b, v in sorted(spf.items())}, **env}
+
+
+# Smallest block size whose products the mixed kernel runs on the int8 tensor
+# cores (the library's cut-over; smaller blocks keep FP64 DMMA products).
+MIXED_MIN_B = 256
+INT8_PEAK_TOPS = 4500.0  # nominal dense int8 rate of a B200 (no measured figure on this pool)
+
+
+def tensor_work(spec, precision, digits):
+    """Work the batched schedule issues per pass, by pipe: int8 tensor-core ops
+    of the Ozaki products (S(S+1)/2 digit pairs, each a real (2b) x b x (2b)
+    product, 2 ops per multiply-add; 6 (n-1) products per instance), and FP64
+    flops on DMMA (every block inverse, b^3 complex multiply-adds, and the
+    products of blocks the mixed path leaves in FP64)."""
+    int8, fp64 = 0.0, 0.0
+    pairs = digits * (digits + 1) // 2
+    for (_, n, b, _) in spec:
+        prods = 6 * (n - 1)
+        fp64 += 8.0 * n * b ** 3
+        if precision == "mixed" and b >= MIXED_MIN_B:
+            int8 += prods * pairs * 2.0 * (2 * b) * b * (2 * b)
+        else:
+            fp64 += prods * 8.0 * b ** 3
+    return int8, fp64
 
 
 # --------------------------------------------------------------------------- arms
+def pipe_rates(spec, args, ms, dmma_peak):
+    """Average rates of the two tensor pipes over one pass (counted work /
+    device time of the pass)."""
+    if ms <= 0:
+        return None
+    int8, fp64 = tensor_work(spec, args.precision, args.digits)
+    sec = ms * 1e-3
+    out = {"dmma": {"tflops": fp64 / sec / 1e12, "frac_of_dmma_peak": fp64 / sec / 1e12 / dmma_peak,
+                    "work": "every block inverse (b^3 complex multiply-adds) and the products left in FP64"}}
+    if int8:
+        out["int8"] = {"tops": int8 / sec / 1e12, "peak_tops": INT8_PEAK_TOPS,
+                       "frac": int8 / sec / 1e12 / INT8_PEAK_TOPS, "peak_source": "nominal dense int8",
+                       "work": "Ozaki digit-pair products, %d pairs of a (2b) x b x (2b) real product each"
+                               % (args.digits * (args.digits + 1) // 2)}
+    return out
+
+
 def run_reference(args, rank, world):
+    """CPU reference arm: the reference RGF on the host cores.  A step is one
+    instance of the fixed stratified sample (cycling through it), timed on
+    the wall clock; ``ms_per_step`` is the median step actually timed.  The
+    matrices/s of the whole batch is extrapolated from the median seconds per
+    canonical flop of each block size over the timed steps."""
     if rank != 0:
         return
+    from oracle import rgf_oracle
+    from sinv_b200 import workloads
     shape = tuple(int(x) for x in args.shape.split(",")) if args.shape else None
     spec = batch_spec(args.count, 0, shape)
-    vals = []
+    idx = cpu_sample(spec)
+    inst = {}
+    spf, steps_ms = {}, []
     for step in range(args.warmup + args.steps):
-        cb = cpu_baseline(spec)
+        k = idx[step % len(idx)]
+        e, n, b, s = spec[k]
+        if k not in inst:
+            inst[k] = workloads.tight_binding(n, b, e, seed=s)
+        t0 = time.perf_counter()
+        rgf_oracle.rgf(*inst[k])
+        t = time.perf_counter() - t0
         if step >= args.warmup:
-            vals.append(cb["value"])
-    v = statistics.median(vals)
-    cb["value"] = v
+            steps_ms.append(1e3 * t)
+            spf.setdefault(b, []).append(t / workloads.rgf_flops(n, b))
+    # block sizes no timed step reached (very short runs) take the nearest timed rate by flops
+    for b in sorted({x[2] for x in spec}):
+        if b not in spf:
+            near = min(spf, key=lambda x: abs(x - b))
+            spf[b] = spf[near]
+    spf_med = {b: statistics.median(v) for b, v in spf.items()}
+    v = len(spec) / _extrapolate(spec, spf_med)
+    env = _cpu_env()
+    cb = {"value": v, "unit": UNIT, "cores": env["blas_threads"], "kind": "port",
+          "sample": "reference rgf (numpy/OpenBLAS restatement of rgf.py, the reference itself cannot run "
+                    "without its sources) on the fixed stratified sample (first %d instances of each block size), "
+                    "one instance per step, %d timed steps after %d warm-up steps; the batch's matrices/s "
+                    "extrapolated from the median seconds per canonical flop of each block size"
+                    % (PER_B, args.steps, args.warmup),
+          "extrapolated": True,
+          "spread_seconds_per_flop": {str(b): [min(x), max(x)] for b, x in sorted(spf.items())}, **env}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * args.count / v,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(steps_ms),
+            "ms_per_step_meaning": "median wall time of one timed step (one sample instance), not of a batch",
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
             "data": "synthetic", "config": {"workload": WORKLOAD, "count": args.count,
                                             "block_sizes": [64, 128, 256, 512], "n_range": [16, 128]},
@@ -346,9 +442,12 @@ def run_sinvb(args, rank, world, local_rank):
            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                         "frac": achieved / peak, "traffic": None,
                         "kernel": "rgf_batched_kernel", "flops": "canonical 8 b^3 (8(n-1)+n) per instance",
+                        "frac_meaning": "FP64-equivalent: canonical flops per second over the FP64 DMMA peak; "
+                                        "the tensor pipes actually used are in pipes",
                         "peak_source": "FP64 tensor-core (DMMA) rate measured at start on this GPU by "
                                        "sinvb_fp64_mma_peak (MEASURED_PEAKS.json has no FP64 figure)",
-                        "peak_dgemm_cublas": dgemm_peak},
+                        "peak_dgemm_cublas": dgemm_peak,
+                        "pipes": pipe_rates(spec, args, sum(kern_ms) / max(1, args.steps), peak)},
            "clocks": clk}
 
     # the plain per-matrix FP64 path (one library call per instance, the whole
@@ -640,7 +739,9 @@ def run_plain_large(args, rank, world, local_rank):
            "roofline": {"bound": "tensor", "achieved": F / (ms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
                         "frac": F / (ms * 1e-3) / 1e12 / peak, "traffic": None, "kernel": "rgf_grid_kernel",
                         "flops": "canonical 8 b^3 (8(n-1)+n)", "peak_source": "sinvb_fp64_mma_peak (DMMA)"},
-           "bcr": {"ms": statistics.median(tb), "matrices_per_s": world / (statistics.median(tb) * 1e-3)},
+           "bcr": {"ms": statistics.median(tb), "matrices_per_s": world / (statistics.median(tb) * 1e-3),
+                   "rel_err_vs_oracle": max(float(np.linalg.norm(g.cpu().numpy() - r) / np.linalg.norm(r))
+                                            for g, r in zip(bcr_s.bcr_blocks(d, u, l), R))},
            "rgf2sided": {"ms": statistics.median(t2), "matrices_per_s": world / (statistics.median(t2) * 1e-3),
                          "rel_err_vs_oracle": max(float(np.linalg.norm(g.cpu().numpy() - r) / np.linalg.norm(r))
                                                   for g, r in zip(rgf2s.rgf2sided(d, u, l), R))},
@@ -853,10 +954,13 @@ def run_gradient_set(args, rank, world, local_rank):
 
 
 def run_large_mixed(args, rank, world, local_rank):
-    """Instances n=256, b=1024 (12.85 GB of input each), tight-binding generator;
-    one wave of `count` instances in place in HBM, mixed precision.  Error of
-    the mixed path on a 4-block sub-instance (n=4, b=1024) against the FP64
-    path and the dense FP64 inverse."""
+    """Instances n=256, b=1024 (12.85 GB of input each), tight-binding generator,
+    mixed precision: 64 instances streamed through HBM in waves (as many as
+    fit in place, 13 on a B200); each wave's inputs are generated on the
+    device (untimed) and one persistent launch inverts the wave (timed).  A
+    step is one pass over all instances.  The FP64 path runs the first wave
+    once for comparison.  Error of the mixed path on a 4-block sub-instance
+    (n=4, b=1024) against the FP64 path and the dense FP64 inverse."""
     import torch
     from sinv_b200 import workloads
     from sinv_b200.algorithms import BatchPlan
@@ -866,34 +970,50 @@ def run_large_mixed(args, rank, world, local_rank):
     if rank:
         spec = [(e, n, b, s + 100000 * rank) for (e, n, b, s) in spec]
     peak = dmma_peak_tflops(torch)
-    pool = torch.empty(sum(in_elems(n, b) for (_, n, b, _) in spec), dtype=torch.complex128, device=dev)
-    views = carve(pool, spec, list(range(len(spec))))
-    plans = {"mixed": BatchPlan(views, precision="mixed", inplace=True, digits=args.digits)}
+    free, _ = torch.cuda.mem_get_info()
+    per = in_elems(spec[0][1], spec[0][2])
+    wave = max(1, min(len(spec), int((free - 8e9) / 16) // per))
+    waves = [list(range(i, min(i + wave, len(spec)))) for i in range(0, len(spec), wave)]
+    pool = torch.empty(wave * per, dtype=torch.complex128, device=dev)
+    views = carve(pool, [spec[0]] * wave, list(range(wave)))
+    plans = {}
 
-    def generate():
-        for (e, n, b, s), (d, u, l) in zip(spec, views):
+    def plan_for(w, precision):
+        key = (len(w), precision)
+        if key not in plans:
+            plans[key] = BatchPlan(views[:len(w)], precision=precision, inplace=True, digits=args.digits)
+        return plans[key]
+
+    def generate(w):
+        for k, (d, u, l) in zip(w, views):
+            e, n, b, s = spec[k]
             workloads.tight_binding_device(n, b, e, s, device=dev, out=(d, u, l))
 
     stream = torch.cuda.current_stream()
     clocks = Clocks(local_rank) if rank == 0 else None
     tm = []
     for step in range(args.warmup + args.steps):
-        generate()
-        torch.cuda.synchronize()
         if step == args.warmup and clocks:
             clocks.start()
-        ms = _events_ms(torch, lambda: plans["mixed"].run(stream), stream)
+        total = 0.0
+        for w in waves:
+            generate(w)
+            torch.cuda.synchronize()
+            p = plan_for(w, "mixed")
+            ms = _events_ms(torch, lambda: p.run(stream), stream)
+            p.check()
+            total += _max_over_ranks(torch, world, dev, ms)
         if step >= args.warmup:
-            tm.append(_max_over_ranks(torch, world, dev, ms))
+            tm.append(total)
     clk = clocks.stop() if clocks else None
-    plans["mixed"].check()
-    del plans["mixed"]
-    plans["fp64"] = BatchPlan(views, precision="fp64", inplace=True)
-    generate()
+    plans.clear()
+    p64 = BatchPlan(views[:len(waves[0])], precision="fp64", inplace=True)
+    generate(waves[0])
     torch.cuda.synchronize()
-    t64 = _events_ms(torch, lambda: plans["fp64"].run(stream), stream)
-    plans["fp64"].check()
-    del plans, views, pool
+    t64 = _events_ms(torch, lambda: p64.run(stream), stream)
+    p64.check()
+    t64_per_inst = t64 / len(waves[0])
+    del p64, views, pool
     torch.cuda.empty_cache()
     # error on the 4-block sub-instance
     e, _, b, sd = spec[0]
@@ -927,9 +1047,11 @@ def run_large_mixed(args, rank, world, local_rank):
             "data": "synthetic",
             "config": {"workload": "large_mixed_%dx(n=256,b=1024)" % len(spec), "count": len(spec),
                        "input_gb": round(sum(in_elems(n, b) for (_, n, b, _) in spec) * 16 / 1e9, 1),
+                       "waves": len(waves), "wave_instances": wave,
                        "in_place": True, "digits": args.digits, "parallelism": "replicas%d" % world},
-            "gpu_launches": args.steps,
-            "fp64_same_wave": {"ms": t64, "matrices_per_s": len(spec) / (t64 * 1e-3), "mixed_over_fp64": t64 / ms},
+            "gpu_launches": args.steps * len(waves),
+            "fp64_first_wave": {"ms": t64, "instances": len(waves[0]), "matrices_per_s": 1e3 / t64_per_inst,
+                                "mixed_over_fp64": t64_per_inst / (ms / len(spec))},
             "rel_err": {"mixed_vs_fp64_sub_instance": err_fp64, "mixed_diag_vs_dense_fp64_inverse": err_dense,
                         "sub_instance": "n=4, b=1024, first instance's generator"},
             "roofline": {"bound": "tensor", "achieved": F / (ms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s (FP64-equivalent)",
@@ -1003,7 +1125,7 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if not args.count:
-        args.count = {"energy_batch": 512, "gradient_set": 128, "large_mixed": 13, "plain_large": 1,
+        args.count = {"energy_batch": 512, "gradient_set": 128, "large_mixed": 64, "plain_large": 1,
                       "bcr_batch": 256}[args.workload]
     if args.impl == "reference":
         if args.workload == "energy_batch":
