@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--tune", dest="tune", action="store_true", default=True,
+                    help="teams, int8 cut-over and queue order from the autotuner (default)")
+    ap.add_argument("--no-tune", dest="tune", action="store_false", help="the library's fixed rule instead")
     return ap.parse_args()
 
 
@@ -288,6 +291,15 @@ def tensor_work(spec, precision, digits):
 
 
 # --------------------------------------------------------------------------- arms
+def schedule_summary(sched):
+    """The autotuner's choices for the bench line: teams used per block size,
+    the int8 cut-over and the estimate."""
+    if not sched:
+        return "fixed rule (teams by block size, int8 products from b=256)"
+    return {"int8_cutover_b": sched.get("int8_cutover"), "estimate_ms": round(sched["estimate_ms"], 1),
+            "teams_used": sorted({int(t) for t in sched["team"]})}
+
+
 def pipe_rates(spec, args, ms, dmma_peak):
     """Average rates of the two tensor pipes over one pass (counted work /
     device time of the pass)."""
@@ -371,6 +383,11 @@ def run_sinvb(args, rank, world, local_rank):
     dgemm_peak = fp64_peak_tflops(torch)
     peak = dmma_peak_tflops(torch)
 
+    if args.tune:  # measure (or load) the autotuner's table before the input pool takes HBM
+        from sinv_b200 import autotune
+        for prec in {args.precision, "fp64"}:
+            autotune.load_or_measure(sorted({b for (_, _, b, _) in spec}), prec, args.digits, dev)
+        torch.cuda.empty_cache()
     free, _ = torch.cuda.mem_get_info()
     # In place (results over the inputs): the whole batch fits in HBM as one
     # wave; the per-CTA scratch slots need ~3 GB more.
@@ -384,7 +401,8 @@ def run_sinvb(args, rank, world, local_rank):
     pool_elems = max(sum(in_elems(spec[k][1], spec[k][2]) for k in w) for w in waves)
     pin = torch.empty(pool_elems, dtype=torch.complex128, device=dev)
     views = [carve(pin, spec, w) for w in waves]
-    plans = [BatchPlan(v, precision=args.precision, inplace=True, digits=args.digits) for v in views]
+    plans = [BatchPlan(v, precision=args.precision, inplace=True, digits=args.digits, tune=args.tune)
+             for v in views]
     flops = [sum(workloads.rgf_flops(spec[k][1], spec[k][2]) for k in w) for w in waves]
 
     def generate(wi):
@@ -436,7 +454,7 @@ def run_sinvb(args, rank, world, local_rank):
            "config": {"workload": workload, "count": args.count, "block_sizes": [64, 128, 256, 512],
                       "n_range": [16, 128], "precision": args.precision, "path": "batched persistent",
                       "waves": len(waves), "wave_input_gb": round(pool_elems * 16 / 1e9, 2),
-                      "in_place": True,
+                      "in_place": True, "schedule": schedule_summary(plans[0].schedule),
                       "l2": "inputs larger than L2 in every wave", "parallelism": "replicas%d" % world},
            "gpu_launches": len(plans) * args.steps,
            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -460,7 +478,7 @@ def run_sinvb(args, rank, world, local_rank):
     # the batched FP64 path over the same batch, one pass (for the mixed line)
     if args.precision != "fp64":
         del plans
-        plans = [BatchPlan(v, precision="fp64", inplace=True) for v in views]
+        plans = [BatchPlan(v, precision="fp64", inplace=True, tune=args.tune) for v in views]
         f_ms = 0.0
         for wi, plan in enumerate(plans):
             generate(wi)

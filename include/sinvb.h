@@ -242,6 +242,31 @@ int sinvb_rgf_batched_stream_d(const sinvb_batch_desc* descs, int count, unsigne
 int sinvb_rgf_batched_rerun_z(void* workspace, sinvb_stream_t stream);
 int sinvb_rgf_batched_rerun_d(void* workspace, sinvb_stream_t stream);
 /*
+ * A schedule for the batched call, as the autotuner (sinv_b200/autotune.py)
+ * chooses it from measured per-block-row costs; no reference counterpart
+ * (the reference inverts one matrix per rgf call, rgf.py:17).  Arrays are
+ * indexed like ``descs``; every field may be left 0 / NULL for the
+ * library's rule (teams of 1 / 2 / 4 / 8 CTAs for b < 256 / 256 / 512 / 1024,
+ * queue ordered by b^3 n, int8 products from b = 256 on).
+ */
+typedef struct sinvb_batch_schedule {
+  const int* team;        /* CTAs of each instance's team (0: the rule), at most the SM count */
+  const float* priority;  /* queue order, highest first (NULL: b^3 n) */
+  int mixed_min_b;        /* mixed batches: smallest b with int8 products (0: 256) */
+  int reserved;
+} sinvb_batch_schedule;
+
+size_t sinvb_rgf_batched_sched_workspace_size(const sinvb_batch_desc* descs, int count, int dtype,
+                                              unsigned flags, const sinvb_batch_schedule* sched);
+/* sinvb_rgf_batched_z / _d with a schedule (NULL: as without). */
+int sinvb_rgf_batched_sched_z(const sinvb_batch_desc* descs, int count, unsigned flags,
+                              const sinvb_batch_schedule* sched, void* workspace, size_t workspace_bytes,
+                              int* status, sinvb_stream_t stream);
+int sinvb_rgf_batched_sched_d(const sinvb_batch_desc* descs, int count, unsigned flags,
+                              const sinvb_batch_schedule* sched, void* workspace, size_t workspace_bytes,
+                              int* status, sinvb_stream_t stream);
+
+/*
  * No reference counterpart (the reference has no device waits; its failure
  * analogue is LinAlgError from rgf.py:44,48).  Bound, in seconds, of every
  * device-side wait of the batched launches that use ``workspace`` from now

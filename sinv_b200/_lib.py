@@ -58,6 +58,9 @@ SIGNATURES = {
     "sinvb_rgf_batched_rerun_z": (_i, [_vp, _vp]),
     "sinvb_rgf_batched_rerun_d": (_i, [_vp, _vp]),
     "sinvb_rgf_batched_set_wait_limit": (_i, [_vp, ctypes.c_double]),
+    "sinvb_rgf_batched_sched_workspace_size": (_sz, [_vp, _i, _i, _u, _vp]),
+    "sinvb_rgf_batched_sched_z": (_i, [_vp, _i, _u, _vp, _vp, _sz, _vp, _vp]),
+    "sinvb_rgf_batched_sched_d": (_i, [_vp, _i, _u, _vp, _vp, _sz, _vp, _vp]),
     "sinvb_rgf_z_noalloc": (_i, [_vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _vp]),
     "sinvb_rgf_checkpoints": (_i, [_i, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "sinvb_rgf_forward_ckpt_z": (_i, [_vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _i, _vp, _sz, _vp]),
@@ -95,6 +98,11 @@ class BatchDesc(ctypes.Structure):
     """``sinvb_batch_desc`` of include/sinvb.h."""
     _fields_ = [("diag", _vp), ("upper", _vp), ("lower", _vp), ("G_diag", _vp), ("G_upper", _vp),
                 ("G_lower", _vp), ("n", _i), ("b", _i)]
+
+
+class BatchSchedule(ctypes.Structure):
+    """``sinvb_batch_schedule`` of include/sinvb.h."""
+    _fields_ = [("team", _vp), ("priority", _vp), ("mixed_min_b", _i), ("reserved", _i)]
 
 
 class SinvbUnavailable(RuntimeError):

@@ -34,6 +34,13 @@ class BatchPlan:
     allocating one when it is large enough (``workspace_bytes``); plans that
     share one must run in order on one stream.
 
+    ``schedule`` (optional): the team of every instance, the queue order and
+    the int8 cut-over, as a dict {"team": [...], "priority": [...],
+    "mixed_min_b": int} (any key may be left out); ``tune=True`` derives it
+    from the autotuner's measured table for this GPU (``sinv_b200.autotune``,
+    cached on disk; the first call for a block size measures it) and keeps
+    the choice in ``self.schedule``.
+
     ``wait_limit`` (seconds, optional): bound of every device-side wait of
     this plan's launches (team barriers, scratch slots, streamed ready
     words; default 60 s).  An instance whose wait runs out gets status
@@ -50,7 +57,8 @@ class BatchPlan:
     """
 
     def __init__(self, instances, sym_mat=False, save_off_diag=True, precision="fp64", outputs=None,
-                 device=None, inplace=False, team=None, digits=7, workspace=None, wait_limit=None):
+                 device=None, inplace=False, team=None, digits=7, workspace=None, wait_limit=None,
+                 schedule=None, tune=False):
         torch = dev._torch()
         self.lib = _lib.load()
         if len(instances) == 0:
@@ -114,8 +122,16 @@ class BatchPlan:
                                       Gl.data_ptr() if (save_off_diag and n > 1) else None, n, b)
         self.descs = descs
         self.device = self.inputs[0][0].device
-        nbytes = self.lib.sinvb_rgf_batched_workspace_size(ctypes.cast(descs, ctypes.c_void_p), len(descs),
-                                                           self.code, self.flags)
+        if tune and schedule is None:
+            from .. import autotune
+            table = autotune.load_or_measure(sorted({b for _, b in self.shapes}), precision, int(digits),
+                                             self.device)
+            sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+            schedule = autotune.schedule(self.shapes, table, sms, precision)
+        self.schedule = schedule
+        self._sched = self._schedule_struct(schedule)
+        nbytes = self.lib.sinvb_rgf_batched_sched_workspace_size(ctypes.cast(descs, ctypes.c_void_p), len(descs),
+                                                                 self.code, self.flags, self._sched_ptr())
         with torch.cuda.device(self.device):
             if workspace is not None and workspace.numel() >= nbytes and workspace.data_ptr() % 256 == 0:
                 self.ws = workspace  # shared with other plans run in order on one stream
@@ -130,6 +146,27 @@ class BatchPlan:
         """Bound (seconds) of every device wait of this plan's later launches."""
         _lib.check(self.lib.sinvb_rgf_batched_set_wait_limit(dev.ptr(self.ws), float(seconds)),
                    "sinvb_rgf_batched_set_wait_limit")
+
+    def _schedule_struct(self, schedule):
+        """ctypes sinvb_batch_schedule for `schedule` (None: no schedule)."""
+        if schedule is None:
+            return None
+        count = len(self.shapes)
+        st = _lib.BatchSchedule()
+        self._sched_arrays = []
+        if schedule.get("team") is not None:
+            team = (ctypes.c_int * count)(*[int(t) for t in schedule["team"]])
+            self._sched_arrays.append(team)
+            st.team = ctypes.cast(team, ctypes.c_void_p)
+        if schedule.get("priority") is not None:
+            prio = (ctypes.c_float * count)(*[float(p) for p in schedule["priority"]])
+            self._sched_arrays.append(prio)
+            st.priority = ctypes.cast(prio, ctypes.c_void_p)
+        st.mixed_min_b = int(schedule.get("mixed_min_b") or 0)
+        return st
+
+    def _sched_ptr(self):
+        return ctypes.cast(ctypes.pointer(self._sched), ctypes.c_void_p) if self._sched is not None else None
 
     @staticmethod
     def workspace_bytes(shapes, dtype_code=None, flags=None, sym_mat=False, save_off_diag=True, precision="fp64",
@@ -158,9 +195,10 @@ class BatchPlan:
         with torch.cuda.device(self.device):
             h = dev.stream_handle(stream)
             if not self.uploaded:
-                fn = self.lib.sinvb_rgf_batched_z if self.code == _lib.C128 else self.lib.sinvb_rgf_batched_d
-                rc = fn(ctypes.cast(self.descs, ctypes.c_void_p), len(self.descs), self.flags, dev.ptr(self.ws),
-                        self.ws.numel(), dev.ptr(self.status_dev), h)
+                fn = self.lib.sinvb_rgf_batched_sched_z if self.code == _lib.C128 else \
+                    self.lib.sinvb_rgf_batched_sched_d
+                rc = fn(ctypes.cast(self.descs, ctypes.c_void_p), len(self.descs), self.flags, self._sched_ptr(),
+                        dev.ptr(self.ws), self.ws.numel(), dev.ptr(self.status_dev), h)
                 _lib.check(rc, "sinvb_rgf_batched")
                 self.uploaded = True
             else:

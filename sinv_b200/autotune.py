@@ -1,0 +1,241 @@
+"""Autotuner of the batched persistent RGF: per block size, which team size
+(CTAs per instance) and which product path (int8 tensor cores or FP64 DMMA)
+run fastest on this GPU, measured and cached; and per batch, the team of
+every instance and the queue order that minimise the estimated makespan.
+
+The reference inverts one matrix per ``rgf`` call
+(``src/sinv/algorithms/rgf/rgf.py:17-64``) and has nothing to tune; the
+batched kernel walks the same 6-product sweep per block row
+(``rgf.py:47-62``) on a team of CTAs, and the cost of a block row depends on
+the block size, the team and the product path:
+
+* a larger team shortens an instance's chain (each product's tiles and each
+  inversion panel's column blocks are split over more CTAs) but costs more
+  SM time per block row (barriers, pivot blocks inverted by every member);
+* int8 products pay digit slicing and pipeline fill, which small blocks do
+  not amortise.
+
+``measure`` times uniform batches that fill the GPU (one instance per team
+slot) and records, per (block size, team, path), the block-row latency with
+the GPU full and the SM time per block row.  ``schedule`` turns that table
+into a ``sinvb_batch_schedule``: every instance starts on its cheapest team
+(least SM time per row); while the longest estimated chain exceeds the
+work bound (total SM time / SMs), that instance moves to the next larger
+team that shortens it; instances are queued longest first.  The int8
+cut-over is the smallest block size whose int8 rows beat its FP64 rows.
+
+The GEMM tile shape follows the block size (32 x 32 tiles for b <= 32,
+64 x 64 above: one tile column per 64-wide inversion panel), so it is not a
+free knob here.
+
+Cache: JSON at ``$SINVB_TUNE_CACHE`` (default
+``~/.cache/sinv_b200/autotune.json``), keyed by device name, SM count,
+library version, precision and digits.
+"""
+
+import json
+import os
+import time
+
+TEAMS = (1, 2, 4, 8)
+FORMAT = 1
+
+
+def cache_path():
+    return os.environ.get("SINVB_TUNE_CACHE") or os.path.join(os.path.expanduser("~"), ".cache", "sinv_b200",
+                                                              "autotune.json")
+
+
+def cache_key(device_name, sms, version, precision, digits):
+    return "%s|sm%d|v%d|%s|d%d" % (device_name, sms, version, precision, digits if precision == "mixed" else 0)
+
+
+def load_cache(path=None):
+    path = path or cache_path()
+    try:
+        with open(path) as f:
+            data = json.load(f)
+        if data.get("format") != FORMAT:
+            return {"format": FORMAT, "entries": {}}
+        return data
+    except (OSError, ValueError):
+        return {"format": FORMAT, "entries": {}}
+
+
+def save_cache(data, path=None):
+    path = path or cache_path()
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def validate_table(table):
+    """A measured table: {"b": {"<team>": {"fp64": {...}, "int8": {...}}}} with
+    row_ms and sm_ms per entry.  Raises ValueError when malformed."""
+    if not isinstance(table, dict) or not table:
+        raise ValueError("empty table")
+    for b, teams in table.items():
+        int(b)
+        if not isinstance(teams, dict) or not teams:
+            raise ValueError("block size %s has no teams" % b)
+        for t, paths in teams.items():
+            if int(t) < 1:
+                raise ValueError("team %s" % t)
+            for path, v in paths.items():
+                if path not in ("fp64", "int8"):
+                    raise ValueError("path %s" % path)
+                if not (v["row_ms"] > 0 and v["sm_ms"] > 0):
+                    raise ValueError("costs of b=%s team=%s %s" % (b, t, path))
+    return table
+
+
+def _rows(b):
+    return 12 if b >= 512 else 16 if b >= 256 else 24
+
+
+def measure(block_sizes, precision="mixed", digits=7, device=None, teams=TEAMS, int8_from=128, log=None):
+    """Measure the block-row costs of every (block size, team, path) on the GPU.
+
+    For each combination a uniform tight-binding batch of grid / team
+    instances (n = 12..24 blocks) runs once untimed and once timed (CUDA
+    events); row_ms = time / n (a block row of one instance with the GPU
+    full), sm_ms = row_ms * team."""
+    import torch
+
+    from . import _lib, workloads
+    from .algorithms import BatchPlan
+
+    device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    table = {}
+    for b in sorted(block_sizes):
+        n = _rows(b)
+        table[str(b)] = {}
+        for t in teams:
+            if t > 1 and t > max(1, b // 64):
+                continue  # more CTAs than 64-wide column blocks: no work for the extra members
+            count = max(1, sms // t)
+            paths = ["fp64"]
+            if precision == "mixed" and b >= int8_from:
+                paths.append("int8")
+            entry = {}
+            for path in paths:
+                inst = [workloads.tight_binding_device(n, b, 0.3 + 0.01 * k, 5000 + k, device=device)
+                        for k in range(count)]
+                # in a mixed batch FP64-product instances run in the mixed kernel:
+                # measure them there (int8 cut-over above b)
+                sched = {"team": [t] * count, "mixed_min_b": (b if path == "int8" else b + 1)}
+                plan = BatchPlan(inst, precision=precision, inplace=True, digits=digits, schedule=sched)
+                plan.run()
+                torch.cuda.synchronize(device)
+                plan.check()
+                for k, (d, u, l) in enumerate(inst):
+                    workloads.tight_binding_device(n, b, 0.3 + 0.01 * k, 5000 + k, device=device, out=(d, u, l))
+                e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+                e0.record()
+                plan.run()
+                e1.record()
+                e1.synchronize()
+                plan.check()
+                ms = e0.elapsed_time(e1)
+                entry[path] = {"row_ms": ms / n, "sm_ms": ms / n * t, "count": count, "n": n}
+                if log:
+                    log("tune b=%d team=%d %s: %.3f ms/row, %.2f SM-ms/row" % (b, t, path, ms / n, ms / n * t))
+                del plan, inst
+                torch.cuda.empty_cache()
+            table[str(b)][str(t)] = entry
+    _ = _lib  # the library is loaded by BatchPlan
+    return validate_table(table)
+
+
+def load_or_measure(block_sizes, precision="mixed", digits=7, device=None, path=None, log=None):
+    """The cached table for this GPU / library / precision, measuring the
+    block sizes it lacks."""
+    import torch
+
+    from . import _lib
+
+    device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    props = torch.cuda.get_device_properties(device)
+    key = cache_key(props.name, props.multi_processor_count, int(_lib.load().sinvb_version()), precision, digits)
+    data = load_cache(path)
+    table = dict(data["entries"].get(key, {}).get("table", {}))
+    missing = [b for b in block_sizes if str(b) not in table]
+    if missing:
+        t0 = time.time()
+        table.update(measure(missing, precision, digits, device, log=log))
+        data["entries"][key] = {"table": table, "measured_at": time.time(), "seconds": time.time() - t0}
+        save_cache(data, path)
+    return validate_table(table)
+
+
+def _best_path(costs):
+    """(path, costs) of the cheaper product path of one team entry."""
+    return min(costs.items(), key=lambda kv: kv[1]["row_ms"])
+
+
+def mixed_cutover(table):
+    """Smallest block size whose int8 rows beat its FP64 rows on its cheapest team."""
+    best = None
+    for b in sorted(table, key=int):
+        teams = table[b]
+        t = min(teams, key=lambda t: _best_path(teams[t])[1]["sm_ms"])
+        paths = teams[t]
+        if "int8" in paths and paths["int8"]["row_ms"] < paths["fp64"]["row_ms"]:
+            best = int(b) if best is None else best
+        elif best is not None:
+            best = None  # int8 must win for every larger block size too
+    return best
+
+
+def _nearest(table, b):
+    keys = sorted(int(x) for x in table)
+    return str(min(keys, key=lambda x: (abs(x - b), x)))
+
+
+def schedule(shapes, table, sms, precision="mixed"):
+    """Teams, queue priorities (estimated ms) and the int8 cut-over for a batch
+    of (n, b) shapes, from a measured table (``measure``).
+
+    Returns {"team": [...], "priority": [...], "mixed_min_b": int,
+    "estimate_ms": float, "work_ms": float, "chain_ms": float}."""
+    cut = mixed_cutover(table) if precision == "mixed" else None
+    mixed_min_b = cut if cut is not None else 1 << 30
+
+    def costs(b, t):
+        row = table[_nearest(table, b)]
+        c = row[str(t)]
+        path = "int8" if (precision == "mixed" and b >= mixed_min_b and "int8" in c) else "fp64"
+        return c[path]
+
+    choices, team = [], []
+    for n, b in shapes:
+        row = table[_nearest(table, b)]
+        ts = sorted((int(t) for t in row), key=int)
+        ts = [t for t in ts if t <= sms]
+        choices.append(ts)
+        team.append(min(ts, key=lambda t: costs(b, t)["sm_ms"]))
+
+    def dur(k):
+        n, b = shapes[k]
+        return (n - 1) * costs(b, team[k])["row_ms"] if n > 1 else costs(b, team[k])["row_ms"]
+
+    def work():
+        return sum(((n - 1) if n > 1 else 1) * costs(b, team[k])["sm_ms"] for k, (n, b) in enumerate(shapes)) / sms
+
+    for _ in range(4 * len(shapes)):
+        k = max(range(len(shapes)), key=dur)
+        if dur(k) <= work():
+            break
+        n, b = shapes[k]
+        bigger = [t for t in choices[k] if t > team[k] and costs(b, t)["row_ms"] < costs(b, team[k])["row_ms"]]
+        if not bigger:
+            break
+        team[k] = min(bigger)
+    durs = [dur(k) for k in range(len(shapes))]
+    never = 1 << 30  # int8 products for no block size
+    return {"team": team, "priority": durs,
+            "mixed_min_b": (int(cut) if cut is not None else never) if precision == "mixed" else 0,
+            "int8_cutover": cut, "estimate_ms": max(work(), max(durs)), "work_ms": work(), "chain_ms": max(durs)}

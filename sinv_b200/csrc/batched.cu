@@ -54,7 +54,8 @@ struct BatchEntry {
   int orig;        // index in the caller's descriptor array
   int team;        // CTAs working on this instance
   int slot_start;  // first queue slot of this instance (entries are in queue order)
-  int pad[3];
+  int int8;        // mixed batches: this instance's products run on the int8 tensor cores
+  int pad[2];
 };
 static_assert(sizeof(BatchEntry<cplx>) == 80, "80-byte entries");
 
@@ -261,9 +262,9 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
     p.flags = flags;
     p.ckpt = nullptr;
     p.ckpt_every = 1;
-    // blocks below kMixedMinB: the int8 path's fixed costs (digit slicing,
-    // pipeline fill) outweigh its faster products, FP64 DMMA is quicker
-    p.oz_digits = e.b >= kMixedMinB ? oz_digits : 0;
+    // small blocks keep FP64 DMMA products: the int8 path's fixed costs
+    // (digit slicing, pipeline fill) outweigh its faster products there
+    p.oz_digits = e.int8 ? oz_digits : 0;
     p.oz_scratch = slot + fp64_slot_bytes(e.n, e.b, sizeof(T), save);
     p.oz = &oz_state;
     if (e.b <= 32)
@@ -306,7 +307,11 @@ static int team_size(int b, unsigned flags) {
 // Team of every instance: team_size(b), and when the default teams leave CTAs
 // of the grid idle (few instances), teams of b >= 256 grow to grid / count
 // CTAs, at most b / 64 (one 64-wide tile column each) and 16.
-static std::vector<int> batch_teams(const sinvb_batch_desc* d, int count, unsigned flags, int grid) {
+//
+// A caller's schedule (sinvb_batch_schedule, e.g. from the autotuner) sets
+// the team of any instance it names instead.
+static std::vector<int> batch_teams(const sinvb_batch_desc* d, int count, unsigned flags, int grid,
+                                    const sinvb_batch_schedule* sched = nullptr) {
   std::vector<int> t(count);
   long total = 0;
   for (int k = 0; k < count; k++) total += t[k] = team_size(d[k].b, flags);
@@ -315,22 +320,32 @@ static std::vector<int> batch_teams(const sinvb_batch_desc* d, int count, unsign
     for (int k = 0; k < count; k++)
       if (d[k].b >= 256) t[k] = std::max(t[k], std::min({share, d[k].b / 64, 16}));
   }
+  if (sched && sched->team)
+    for (int k = 0; k < count; k++)
+      if (sched->team[k] > 0) t[k] = std::min(sched->team[k], grid);
   return t;
 }
 
-static BatchLayout batch_layout(const sinvb_batch_desc* d, int count, int dtype, unsigned flags) {
+// Smallest block size whose products a mixed batch runs on the int8 tensor cores.
+static int mixed_min_b(const sinvb_batch_schedule* sched) {
+  return sched && sched->mixed_min_b > 0 ? sched->mixed_min_b : kMixedMinB;
+}
+
+static BatchLayout batch_layout(const sinvb_batch_desc* d, int count, int dtype, unsigned flags,
+                                const sinvb_batch_schedule* sched = nullptr) {
   BatchLayout L{};
   const size_t es = elem_bytes(dtype);
   const bool save = flags & SINVB_SAVE_OFFDIAG;
   const bool mixed = flags & SINVB_PREC_MIXED;
+  const int min_b = mixed_min_b(sched);
   size_t slot = 0;
   for (int k = 0; k < count; k++) {
     size_t s = fp64_slot_bytes(d[k].n, d[k].b, es, save);
-    if (mixed && d[k].b >= kMixedMinB) s += 2 * oz_op_scratch(d[k].b, d[k].b, d[k].b, mixed_digits(flags));
+    if (mixed && d[k].b >= min_b) s += 2 * oz_op_scratch(d[k].b, d[k].b, d[k].b, mixed_digits(flags));
     slot = std::max(slot, s);
   }
   // scratch slots: as many as teams can run at once (grid / smallest team)
-  const std::vector<int> teams = batch_teams(d, count, flags, (int)batch_slots());
+  const std::vector<int> teams = batch_teams(d, count, flags, (int)batch_slots(), sched);
   const int min_team = *std::min_element(teams.begin(), teams.end());
   L.nslots = std::min<unsigned>(batch_slots() / min_team, 256u);
   L.desc_offset = sizeof(WsHeader);
@@ -342,8 +357,14 @@ static BatchLayout batch_layout(const sinvb_batch_desc* d, int count, int dtype,
 }
 
 static int check_batch(const sinvb_batch_desc* d, int count, unsigned flags, const void* ws, size_t ws_bytes,
-                       int dtype) {
+                       int dtype, const sinvb_batch_schedule* sched = nullptr) {
   if (!d || count < 1 || !ws) return SINVB_EINVAL;
+  if (sched) {
+    if (sched->mixed_min_b < 0) return SINVB_EINVAL;
+    if (sched->team)
+      for (int k = 0; k < count; k++)
+        if (sched->team[k] < 0 || sched->team[k] > (int)batch_slots()) return SINVB_EINVAL;
+  }
   if ((uintptr_t)ws % 256) return SINVB_EWORKSPACE;
   const bool save = flags & SINVB_SAVE_OFFDIAG;
   const size_t align = elem_bytes(dtype);
@@ -357,7 +378,7 @@ static int check_batch(const sinvb_batch_desc* d, int count, unsigned flags, con
     for (const void* q : {e.diag, e.upper, e.lower, (const void*)e.G_diag, (const void*)e.G_upper, (const void*)e.G_lower})
       if (q && (uintptr_t)q % align) return SINVB_EINVAL;
   }
-  if (ws_bytes < batch_layout(d, count, dtype, flags).total) return SINVB_EWORKSPACE;
+  if (ws_bytes < batch_layout(d, count, dtype, flags, sched).total) return SINVB_EWORKSPACE;
   return check_device();
 }
 
@@ -390,11 +411,16 @@ static int launch_batched(void* ws, int count, unsigned flags, cudaStream_t stre
 template <class T>
 static int upload_and_run(const sinvb_batch_desc* d, int count, unsigned flags, void* ws, size_t ws_bytes,
                           int* status, cudaStream_t stream, int dtype, const unsigned* ready = nullptr,
-                          unsigned* done = nullptr, unsigned gen = 0) {
-  int rc = check_batch(d, count, flags, ws, ws_bytes, dtype);
+                          unsigned* done = nullptr, unsigned gen = 0, const sinvb_batch_schedule* sched = nullptr) {
+  int rc = check_batch(d, count, flags, ws, ws_bytes, dtype, sched);
   if (rc) return rc;
-  const BatchLayout L = batch_layout(d, count, dtype, flags);
-  const std::vector<int> teams = batch_teams(d, count, flags, (int)batch_slots());
+  const BatchLayout L = batch_layout(d, count, dtype, flags, sched);
+  const std::vector<int> teams = batch_teams(d, count, flags, (int)batch_slots(), sched);
+  const bool mixed = flags & SINVB_PREC_MIXED;
+  const int min_b = mixed_min_b(sched);
+  std::vector<double> prio(count);
+  for (int k = 0; k < count; k++)
+    prio[k] = sched && sched->priority ? (double)sched->priority[k] : (double)d[k].b * d[k].b * d[k].b * d[k].n;
   std::vector<BatchEntry<T>> entries(count);
   for (int k = 0; k < count; k++) {
     BatchEntry<T>& e = entries[k];
@@ -409,11 +435,13 @@ static int upload_and_run(const sinvb_batch_desc* d, int count, unsigned flags, 
     e.orig = k;
     e.team = teams[k];
     e.slot_start = 0;
-    e.pad[0] = e.pad[1] = e.pad[2] = 0;
+    e.int8 = mixed && d[k].b >= min_b;
+    e.pad[0] = e.pad[1] = 0;
   }
-  // largest first (cost ~ b^3 n): long chains start while short ones fill in
-  std::stable_sort(entries.begin(), entries.end(), [](const BatchEntry<T>& x, const BatchEntry<T>& y) {
-    return (double)x.b * x.b * x.b * x.n > (double)y.b * y.b * y.b * y.n;
+  // longest first (by default cost ~ b^3 n; a schedule may give its own
+  // estimates): long chains start while short ones fill in
+  std::stable_sort(entries.begin(), entries.end(), [&](const BatchEntry<T>& x, const BatchEntry<T>& y) {
+    return prio[x.orig] > prio[y.orig];
   });
   int total_slots = 0;
   for (auto& e : entries) {
@@ -505,6 +533,31 @@ int sinvb_rgf_batched_stream_d(const sinvb_batch_desc* descs, int count, unsigne
   if (flags & SINVB_PREC_MIXED) return SINVB_EUNSUPPORTED;
   return upload_and_run<double>(descs, count, flags, workspace, workspace_bytes, status, (cudaStream_t)stream,
                                 SINVB_F64, ready, done, gen);
+}
+
+size_t sinvb_rgf_batched_sched_workspace_size(const sinvb_batch_desc* descs, int count, int dtype, unsigned flags,
+                                              const sinvb_batch_schedule* sched) {
+  if (!descs || count < 1 || dtype < 0 || dtype > 1) return 0;
+  return batch_layout(descs, count, dtype, flags, sched).total;
+}
+
+int sinvb_rgf_batched_sched_z(const sinvb_batch_desc* descs, int count, unsigned flags,
+                              const sinvb_batch_schedule* sched, void* workspace, size_t workspace_bytes, int* status,
+                              sinvb_stream_t stream) {
+  if ((flags & SINVB_PREC_MIXED) && mixed_digits(flags) > kOzMaxDigits) return SINVB_EINVAL;
+  if (flags & SINVB_PREC_MIXED)
+    for (int k = 0; k < count; k++)
+      if (descs && descs[k].b >= mixed_min_b(sched) && 2 * descs[k].b > (1 << 14)) return SINVB_EINVAL;
+  return upload_and_run<cplx>(descs, count, flags, workspace, workspace_bytes, status, (cudaStream_t)stream,
+                              SINVB_C128, nullptr, nullptr, 0, sched);
+}
+
+int sinvb_rgf_batched_sched_d(const sinvb_batch_desc* descs, int count, unsigned flags,
+                              const sinvb_batch_schedule* sched, void* workspace, size_t workspace_bytes, int* status,
+                              sinvb_stream_t stream) {
+  if (flags & SINVB_PREC_MIXED) return SINVB_EUNSUPPORTED;
+  return upload_and_run<double>(descs, count, flags, workspace, workspace_bytes, status, (cudaStream_t)stream,
+                                SINVB_F64, nullptr, nullptr, 0, sched);
 }
 
 int sinvb_rgf_batched_set_wait_limit(const void* workspace, double seconds) {

@@ -46,7 +46,7 @@ int check_device() {
 
 extern "C" {
 
-int sinvb_version(void) { return 100; }
+int sinvb_version(void) { return 110; }
 
 const char* sinvb_status_string(int code) {
   switch (code) {
