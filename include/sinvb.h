@@ -267,6 +267,54 @@ int sinvb_rgf_batched_sched_d(const sinvb_batch_desc* descs, int count, unsigned
                               int* status, sinvb_stream_t stream);
 
 /*
+ * Batched forward sweeps that also save the adjoint's checkpoints (the
+ * batched form of sinvb_rgf_forward_ckpt_*; no reference counterpart, the
+ * reference has no gradients): instance k writes g_{s*c-1}, c =
+ * ceil(sqrt(n_k)), into checkpoints[k], a device array of the count blocks
+ * sinvb_rgf_checkpoints(n_k) gives (NULL allowed when that count is 0).
+ * FP64 products only, not in place.
+ */
+int sinvb_rgf_batched_ckpt_z(const sinvb_batch_desc* descs, int count, unsigned flags, void* const* checkpoints,
+                             void* workspace, size_t workspace_bytes, int* status, sinvb_stream_t stream);
+int sinvb_rgf_batched_ckpt_d(const sinvb_batch_desc* descs, int count, unsigned flags, void* const* checkpoints,
+                             void* workspace, size_t workspace_bytes, int* status, sinvb_stream_t stream);
+
+/*
+ * Batched adjoint: the reverse of both sweeps (rgf.py:44-62) of many
+ * instances in one persistent launch, as sinvb_rgf_adjoint_* for each
+ * (checkpoints from sinvb_rgf_batched_ckpt_* or sinvb_rgf_forward_ckpt_*).
+ * No reference counterpart.  Per instance: inputs A, the forward results G,
+ * upstream adjoints bG (bG_upper / bG_lower may be NULL), checkpoints, and
+ * the outputs aD (n blocks), aU, aL (n-1 blocks).  flags: SINVB_SYM,
+ * SINVB_SAVE_OFFDIAG, SINVB_FORCE_CTA.  ``status``: per-instance device
+ * status (optional).
+ */
+typedef struct sinvb_adjoint_desc {
+  const void* diag;
+  const void* upper;
+  const void* lower;
+  const void* G_diag;
+  const void* G_upper;
+  const void* G_lower;
+  const void* bG_diag;
+  const void* bG_upper;
+  const void* bG_lower;
+  const void* checkpoints;
+  void* aD;
+  void* aU;
+  void* aL;
+  int n;
+  int b;
+} sinvb_adjoint_desc;
+
+size_t sinvb_rgf_adjoint_batched_workspace_size(const sinvb_adjoint_desc* descs, int count, int dtype,
+                                                unsigned flags);
+int sinvb_rgf_adjoint_batched_z(const sinvb_adjoint_desc* descs, int count, unsigned flags, void* workspace,
+                                size_t workspace_bytes, int* status, sinvb_stream_t stream);
+int sinvb_rgf_adjoint_batched_d(const sinvb_adjoint_desc* descs, int count, unsigned flags, void* workspace,
+                                size_t workspace_bytes, int* status, sinvb_stream_t stream);
+
+/*
  * No reference counterpart (the reference has no device waits; its failure
  * analogue is LinAlgError from rgf.py:44,48).  Bound, in seconds, of every
  * device-side wait of the batched launches that use ``workspace`` from now

@@ -61,6 +61,11 @@ SIGNATURES = {
     "sinvb_rgf_batched_sched_workspace_size": (_sz, [_vp, _i, _i, _u, _vp]),
     "sinvb_rgf_batched_sched_z": (_i, [_vp, _i, _u, _vp, _vp, _sz, _vp, _vp]),
     "sinvb_rgf_batched_sched_d": (_i, [_vp, _i, _u, _vp, _vp, _sz, _vp, _vp]),
+    "sinvb_rgf_batched_ckpt_z": (_i, [_vp, _i, _u, _vp, _vp, _sz, _vp, _vp]),
+    "sinvb_rgf_batched_ckpt_d": (_i, [_vp, _i, _u, _vp, _vp, _sz, _vp, _vp]),
+    "sinvb_rgf_adjoint_batched_workspace_size": (_sz, [_vp, _i, _i, _u]),
+    "sinvb_rgf_adjoint_batched_z": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp]),
+    "sinvb_rgf_adjoint_batched_d": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp]),
     "sinvb_rgf_z_noalloc": (_i, [_vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _vp]),
     "sinvb_rgf_checkpoints": (_i, [_i, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "sinvb_rgf_forward_ckpt_z": (_i, [_vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _i, _vp, _sz, _vp]),
@@ -98,6 +103,13 @@ class BatchDesc(ctypes.Structure):
     """``sinvb_batch_desc`` of include/sinvb.h."""
     _fields_ = [("diag", _vp), ("upper", _vp), ("lower", _vp), ("G_diag", _vp), ("G_upper", _vp),
                 ("G_lower", _vp), ("n", _i), ("b", _i)]
+
+
+class AdjointDesc(ctypes.Structure):
+    """``sinvb_adjoint_desc`` of include/sinvb.h."""
+    _fields_ = [(name, _vp) for name in ("diag", "upper", "lower", "G_diag", "G_upper", "G_lower", "bG_diag",
+                                         "bG_upper", "bG_lower", "checkpoints", "aD", "aU", "aL")] + \
+        [("n", _i), ("b", _i)]
 
 
 class BatchSchedule(ctypes.Structure):

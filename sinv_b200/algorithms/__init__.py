@@ -17,6 +17,6 @@ from . import psr_seqsolve as psr_s  # noqa: F401
 from . import batched  # noqa: F401
 from .batched import BatchPlan, rgf_batched, rgf_batched_host  # noqa: F401
 from . import adjoint  # noqa: F401
-from .adjoint import RGFFunction, rgf_autograd  # noqa: F401
+from .adjoint import RGFBatchFunction, RGFFunction, rgf_autograd, rgf_batched_autograd  # noqa: F401
 from . import lesser  # noqa: F401
 from .lesser import rgf_greater, rgf_lesser  # noqa: F401

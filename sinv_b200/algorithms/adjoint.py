@@ -109,3 +109,126 @@ def rgf_autograd(A_diag, A_upper, A_lower, sym_mat=False, team=None):
     the inputs; ``backward`` runs the GPU adjoint.
     """
     return RGFFunction.apply(A_diag, A_upper, A_lower, sym_mat, team)
+
+
+# --------------------------------------------------------------------------- batches
+def _p(x):
+    """Device address of a tensor for a descriptor field (None: absent or empty)."""
+    return x.data_ptr() if x is not None and x.numel() > 0 else None
+
+
+def _forward_batched(instances, sym_mat):
+    """Batched forward with checkpoints: one persistent launch over all
+    instances (``sinvb_rgf_batched_ckpt_*``)."""
+    torch = dev._torch()
+    lib = _lib.load()
+    dt = _wide(torch, instances[0][0].dtype)
+    code = _lib.dtype_code(dt)
+    if code not in (_lib.C128, _lib.F64):
+        raise TypeError("batched autograd takes complex or real floating tensors")
+    flags = _lib.SAVE_OFFDIAG | (_lib.SYM if sym_mat else 0)
+    count = len(instances)
+    descs = (_lib.BatchDesc * count)()
+    cks = (ctypes.c_void_p * count)()
+    saved = []
+    for k, (A_diag, A_upper, A_lower) in enumerate(instances):
+        d = A_diag.detach().to(dt).contiguous()
+        n, b = int(d.shape[0]), int(d.shape[1])
+        u = A_upper.detach().to(dt).contiguous()
+        l = A_lower.detach().to(dt).contiguous()
+        every, nck = _checkpoints(lib, n)
+        Gd, Gu, Gl = torch.empty_like(d), torch.empty_like(u), torch.empty_like(l)
+        ck = torch.empty((max(nck, 1), b, b), dtype=dt, device=d.device)
+        descs[k] = _lib.BatchDesc(_p(d), _p(u), _p(l), _p(Gd), _p(Gu), _p(Gl), n, b)
+        cks[k] = ck.data_ptr()
+        saved.append((d, u, l, Gd, Gu, Gl, ck))
+    device = saved[0][0].device
+    nbytes = lib.sinvb_rgf_batched_workspace_size(ctypes.cast(descs, ctypes.c_void_p), count, code, flags)
+    ws = dev.workspace(nbytes, device)
+    status = torch.zeros(count, dtype=torch.int32, device=device)
+    fn = lib.sinvb_rgf_batched_ckpt_z if code == _lib.C128 else lib.sinvb_rgf_batched_ckpt_d
+    rc = fn(ctypes.cast(descs, ctypes.c_void_p), count, flags, ctypes.cast(cks, ctypes.c_void_p), dev.ptr(ws),
+            ws.numel(), dev.ptr(status), dev.stream_handle())
+    _lib.check(rc, "sinvb_rgf_batched_ckpt")
+    _raise_for_statuses(status, "rgf (batched autograd forward)")
+    return saved, flags
+
+
+def _raise_for_statuses(status, where):
+    st = status.cpu().numpy()
+    bad = [k for k in range(len(st)) if st[k]]
+    if bad:
+        import numpy as np
+        if st[bad[0]] == _lib.STATUS_PIVOT:
+            raise np.linalg.LinAlgError("%s: zero or non-finite pivot in instance %d" % (where, bad[0]))
+        raise RuntimeError("%s: instance %d status %d" % (where, bad[0], st[bad[0]]))
+
+
+def _adjoint_batched(saved, flags, grads):
+    """Batched adjoint (``sinvb_rgf_adjoint_batched_*``): one persistent launch."""
+    torch = dev._torch()
+    lib = _lib.load()
+    count = len(saved)
+    dt = saved[0][0].dtype
+    code = _lib.dtype_code(dt)
+    descs = (_lib.AdjointDesc * count)()
+    outs, keep = [], []
+    for k, ((d, u, l, Gd, Gu, Gl, ck), (bGd, bGu, bGl)) in enumerate(zip(saved, grads)):
+        n, b = int(d.shape[0]), int(d.shape[1])
+        bGd = torch.zeros_like(Gd) if bGd is None else bGd.to(dt).contiguous()
+        bGu = None if bGu is None else bGu.to(dt).contiguous()
+        bGl = None if bGl is None else bGl.to(dt).contiguous()
+        aD, aU, aL = torch.empty_like(d), torch.empty_like(u), torch.empty_like(l)
+        every, nck = _checkpoints(lib, n)
+        descs[k] = _lib.AdjointDesc(_p(d), _p(u), _p(l), _p(Gd), _p(Gu), _p(Gl), _p(bGd), _p(bGu), _p(bGl),
+                                    _p(ck) if nck else None, _p(aD), _p(aU), _p(aL), n, b)
+        keep.append((bGd, bGu, bGl))
+        outs.append((aD, aU, aL))
+    device = saved[0][0].device
+    nbytes = lib.sinvb_rgf_adjoint_batched_workspace_size(ctypes.cast(descs, ctypes.c_void_p), count, code, flags)
+    ws = dev.workspace(nbytes, device)
+    status = torch.zeros(count, dtype=torch.int32, device=device)
+    fn = lib.sinvb_rgf_adjoint_batched_z if code == _lib.C128 else lib.sinvb_rgf_adjoint_batched_d
+    rc = fn(ctypes.cast(descs, ctypes.c_void_p), count, flags, dev.ptr(ws), ws.numel(), dev.ptr(status),
+            dev.stream_handle())
+    _lib.check(rc, "sinvb_rgf_adjoint_batched")
+    _raise_for_statuses(status, "rgf (batched adjoint)")
+    del keep
+    return outs
+
+
+class RGFBatchFunction(torch.autograd.Function):
+    """Many selected inversions with the GPU adjoint, each direction one
+    persistent launch: ``(sym_mat, d_0, u_0, l_0, d_1, ...) -> (G_diag_0,
+    G_upper_0, G_lower_0, ...)``."""
+
+    @staticmethod
+    def forward(ctx, sym_mat, *flat):
+        inst = [tuple(flat[3 * k:3 * k + 3]) for k in range(len(flat) // 3)]
+        saved, flags = _forward_batched(inst, sym_mat)
+        ctx.saved, ctx.flags = saved, flags
+        ctx.in_dtypes = [x.dtype for x in flat]
+        out = []
+        for (d, u, l, Gd, Gu, Gl, ck), (A_d, _, _) in zip(saved, inst):
+            out += [Gd.to(A_d.dtype), Gu.to(A_d.dtype), Gl.to(A_d.dtype)]
+        return tuple(out)
+
+    @staticmethod
+    def backward(ctx, *flat_grads):
+        grads = [tuple(flat_grads[3 * k:3 * k + 3]) for k in range(len(ctx.saved))]
+        outs = _adjoint_batched(ctx.saved, ctx.flags, grads)
+        res = []
+        for (aD, aU, aL), k in zip(outs, range(len(outs))):
+            res += [aD.to(ctx.in_dtypes[3 * k]), aU.to(ctx.in_dtypes[3 * k + 1]), aL.to(ctx.in_dtypes[3 * k + 2])]
+        ctx.saved = None
+        return (None, *res)
+
+
+def rgf_batched_autograd(instances, sym_mat=False):
+    """Differentiable selected inversion of many instances (torch CUDA
+    tensors, each ``(A_diag, A_upper, A_lower)``, own n and b): one batched
+    forward launch, and on ``backward`` one batched adjoint launch.  Returns
+    a list of ``(G_diag, G_upper, G_lower)``."""
+    flat = [x for inst in instances for x in inst]
+    out = RGFBatchFunction.apply(sym_mat, *flat)
+    return [tuple(out[3 * k:3 * k + 3]) for k in range(len(instances))]

@@ -195,47 +195,98 @@ def _nearest(table, b):
     return str(min(keys, key=lambda x: (abs(x - b), x)))
 
 
+def simulate(durations, teams, priority, sms):
+    """Makespan (ms) of the persistent kernel's queue for given per-instance
+    durations (ms with its team), teams and priorities: instances in
+    descending priority, their member slots handed out in order to whichever
+    CTA is free first; an instance starts when its last member has arrived
+    (members that arrive early wait) and holds all its members until it
+    ends."""
+    import heapq
+    order = sorted(range(len(durations)), key=lambda k: -priority[k])
+    free = [(0.0, c) for c in range(sms)]
+    heapq.heapify(free)
+    end = 0.0
+    for k in order:
+        members = [heapq.heappop(free) for _ in range(min(teams[k], sms))]
+        start = max(t for t, _ in members)
+        finish = start + durations[k]
+        end = max(end, finish)
+        for _, c in members:
+            heapq.heappush(free, (finish, c))
+    return end
+
+
+def fixed_rule_teams(shapes, sms):
+    """The library's own team rule (sinvb_rgf_batched_* without a schedule)."""
+    t = [8 if b >= 1024 else 4 if b >= 512 else 2 if b >= 256 else 1 for _, b in shapes]
+    if sum(t) < sms:
+        share = sms // len(shapes)
+        t = [max(x, min(share, b // 64, 16)) if b >= 256 else x for x, (_, b) in zip(t, shapes)]
+    return t
+
+
 def schedule(shapes, table, sms, precision="mixed"):
     """Teams, queue priorities (estimated ms) and the int8 cut-over for a batch
     of (n, b) shapes, from a measured table (``measure``).
 
-    Returns {"team": [...], "priority": [...], "mixed_min_b": int,
-    "estimate_ms": float, "work_ms": float, "chain_ms": float}."""
+    Candidates: the library's fixed rule, every instance on its SM-cheapest
+    team, and the greedy assignment that moves the longest estimated chain to
+    a larger team while it exceeds a fraction of the work bound (several
+    fractions); the candidate with the smallest simulated makespan
+    (``simulate``) wins.  Returns {"team": [...], "priority": [...],
+    "mixed_min_b": int, "int8_cutover": b or None, "estimate_ms": float,
+    "work_ms": float, "chain_ms": float, "candidate": str}."""
     cut = mixed_cutover(table) if precision == "mixed" else None
     mixed_min_b = cut if cut is not None else 1 << 30
 
     def costs(b, t):
         row = table[_nearest(table, b)]
-        c = row[str(t)]
+        key = str(t) if str(t) in row else min(row, key=lambda x: abs(int(x) - t))
+        c = row[key]
         path = "int8" if (precision == "mixed" and b >= mixed_min_b and "int8" in c) else "fp64"
         return c[path]
 
-    choices, team = [], []
+    rows = [(n - 1) if n > 1 else 1 for n, _ in shapes]
+
+    def durations(team):
+        return [r * costs(b, t)["row_ms"] for r, (_, b), t in zip(rows, shapes, team)]
+
+    def work(team):
+        return sum(r * costs(b, t)["sm_ms"] for r, (_, b), t in zip(rows, shapes, team)) / sms
+
+    choices = []
     for n, b in shapes:
         row = table[_nearest(table, b)]
-        ts = sorted((int(t) for t in row), key=int)
-        ts = [t for t in ts if t <= sms]
-        choices.append(ts)
-        team.append(min(ts, key=lambda t: costs(b, t)["sm_ms"]))
+        choices.append(sorted(t for t in (int(x) for x in row) if t <= sms))
+    cheapest = [min(ts, key=lambda t: costs(b, t)["sm_ms"]) for ts, (_, b) in zip(choices, shapes)]
 
-    def dur(k):
-        n, b = shapes[k]
-        return (n - 1) * costs(b, team[k])["row_ms"] if n > 1 else costs(b, team[k])["row_ms"]
+    def greedy(frac):
+        team = list(cheapest)
+        for _ in range(4 * len(shapes)):
+            d = durations(team)
+            k = max(range(len(shapes)), key=lambda i: d[i])
+            if d[k] <= frac * work(team):
+                break
+            b = shapes[k][1]
+            bigger = [t for t in choices[k] if t > team[k] and costs(b, t)["row_ms"] < costs(b, team[k])["row_ms"]]
+            if not bigger:
+                break
+            team[k] = min(bigger)
+        return team
 
-    def work():
-        return sum(((n - 1) if n > 1 else 1) * costs(b, team[k])["sm_ms"] for k, (n, b) in enumerate(shapes)) / sms
-
-    for _ in range(4 * len(shapes)):
-        k = max(range(len(shapes)), key=dur)
-        if dur(k) <= work():
-            break
-        n, b = shapes[k]
-        bigger = [t for t in choices[k] if t > team[k] and costs(b, t)["row_ms"] < costs(b, team[k])["row_ms"]]
-        if not bigger:
-            break
-        team[k] = min(bigger)
-    durs = [dur(k) for k in range(len(shapes))]
+    cands = {"fixed rule": fixed_rule_teams(shapes, sms), "cheapest": cheapest}
+    for frac in (0.5, 0.7, 0.85, 1.0):
+        cands["greedy %.2f" % frac] = greedy(frac)
+    best = None
+    for name, team in cands.items():
+        d = durations(team)
+        span = simulate(d, team, d, sms)
+        if best is None or span < best[0]:
+            best = (span, name, team, d)
+    span, name, team, durs = best
     never = 1 << 30  # int8 products for no block size
     return {"team": team, "priority": durs,
             "mixed_min_b": (int(cut) if cut is not None else never) if precision == "mixed" else 0,
-            "int8_cutover": cut, "estimate_ms": max(work(), max(durs)), "work_ms": work(), "chain_ms": max(durs)}
+            "int8_cutover": cut, "estimate_ms": span, "work_ms": work(team), "chain_ms": max(durs),
+            "candidate": name}

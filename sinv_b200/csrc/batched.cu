@@ -13,10 +13,12 @@
 // Each CTA owns a scratch slot in the workspace (the T / side buffers of the
 // sweep, sized for the largest instance), reused instance after instance.
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
 
+#include "batch_queue.cuh"
 #include "host_util.h"
 #include "rgf_sweep.cuh"
 
@@ -55,7 +57,7 @@ struct BatchEntry {
   int team;        // CTAs working on this instance
   int slot_start;  // first queue slot of this instance (entries are in queue order)
   int int8;        // mixed batches: this instance's products run on the int8 tensor cores
-  int pad[2];
+  T* ckpt;         // optional: checkpoints g_{s c - 1} of the forward sweep for the adjoint
 };
 static_assert(sizeof(BatchEntry<cplx>) == 80, "80-byte entries");
 
@@ -77,105 +79,6 @@ __host__ __device__ inline size_t fp64_slot_bytes(int n, int b, size_t es, bool 
   size_t s = 4 * bb + invert_side_elems(b);
   if (!save) s += 2 * (size_t)(n - 1) * bb;
   return (s * es + 255) / 256 * 256;
-}
-
-// Per-instance meeting point of its team (64 bytes apart).
-struct ItemArea {
-  unsigned counter;  // team barrier arrivals
-  int status;        // device status of the instance
-  unsigned char* scratch;  // scratch slot of the team's rank-0 CTA
-  int slot_id;       // its index in the slot bitmap (-1: none)
-  unsigned left;     // members that have finished with the instance
-  unsigned pad[10];
-};
-static_assert(sizeof(ItemArea) == 64, "64-byte item areas");
-
-// Scratch slots are taken by a team's rank 0 from the bitmap hdr->slot_bits
-// (hdr->nslots slots, at least as many as teams that can run at once, so a
-// slot is normally free at once; the wait is bounded all the same).
-__device__ inline int acquire_scratch(WsHeader* hdr, int* status, unsigned long long wait_ns) {
-  const int K = (int)hdr->nslots;
-  unsigned long long t0 = 0;
-  for (unsigned spins = 0;; spins++) {
-    for (int w = 0; w * 32 < K; w++) {
-      const unsigned valid = (K - w * 32 >= 32) ? 0xffffffffu : ((1u << (K - w * 32)) - 1u);
-      unsigned cur = *((volatile unsigned*)&hdr->slot_bits[w]);
-      while (true) {
-        const unsigned freeb = ~cur & valid;
-        if (!freeb) break;
-        const int bit = __ffs(freeb) - 1;
-        const unsigned old = atomicOr(&hdr->slot_bits[w], 1u << bit);
-        if (!(old & (1u << bit))) return w * 32 + bit;
-        cur = old | (1u << bit);
-      }
-    }
-    __nanosleep(256);
-    if ((spins & 255) == 255) {
-      const unsigned long long now = global_ns();
-      if (t0 == 0) t0 = now;
-      else if (now - t0 > wait_ns) {
-        report(status, SINVB_STATUS_TIMEOUT);
-        return -1;
-      }
-    }
-  }
-}
-// Streamed batches: the inputs of instance k are in place once ready[k]
-// holds this call's generation (written by a copy after the data, in stream
-// order); a bounded wait.  Returns false (timeout reported) when the word
-// never came; the instance is then skipped.
-__device__ inline bool wait_ready(const WsHeader* hdr, int k, int* status, unsigned long long wait_ns) {
-  const unsigned gen = hdr->gen;
-  unsigned long long t0 = 0;
-  for (unsigned spins = 0;; spins++) {
-    unsigned v;
-    asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(hdr->ready + k) : "memory");
-    if (v == gen) return true;
-    __nanosleep(512);
-    if ((spins & 255) == 255) {
-      const unsigned long long now = global_ns();
-      if (t0 == 0) t0 = now;
-      else if (now - t0 > wait_ns) {
-        report(status, SINVB_STATUS_TIMEOUT);
-        return false;
-      }
-    }
-  }
-}
-// ... and done[k] tells the host that instance k's results may be copied out.
-__device__ inline void signal_done(const WsHeader* hdr, int k) {
-  if (!hdr->done) return;
-  __threadfence_system();
-  asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(hdr->done + k), "r"(hdr->gen) : "memory");
-}
-
-__device__ inline void release_scratch(WsHeader* hdr, int id) {
-  if (id < 0) return;
-  __threadfence();
-  atomicAnd(&hdr->slot_bits[id >> 5], ~(1u << (id & 31)));
-}
-
-// Called by thread 0 of every member once its CTA is done with the instance
-// (after a __syncthreads), on every path out of it: the last member to leave
-// returns the scratch slot.  A failed pivot leaves every member running to the
-// sweep's final barrier, a wait that gave up lets members leave at different
-// times; either way the slot comes free only when no member can touch it.
-__device__ inline void leave_item(WsHeader* hdr, ItemArea* item, int team) {
-  __threadfence();
-  if (atomicAdd(&item->left, 1u) == (unsigned)team - 1) {
-    __threadfence();  // rank 0 wrote slot_id before it left
-    const int id = *((volatile int*)&item->slot_id);
-    release_scratch(hdr, id);
-  }
-}
-
-// Thread 0 of rank 0: the instance's status to the caller's array and the
-// call-wide word, and (streamed calls) its done word.
-__device__ inline void finish_item(WsHeader* hdr, ItemArea* item, int orig) {
-  const int st = *((volatile int*)&item->status);
-  if (hdr->inst_status) hdr->inst_status[orig] = st;
-  if (st) report(&hdr->status, st);
-  signal_done(hdr, orig);
 }
 
 // Persistent: every CTA repeatedly takes one queue slot.  Slot s belongs to the
@@ -260,8 +163,8 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_batched_kernel(unsigned char*
     p.n = e.n;
     p.b = e.b;
     p.flags = flags;
-    p.ckpt = nullptr;
-    p.ckpt_every = 1;
+    p.ckpt = e.ckpt;  // c = ceil(sqrt(n)), as the adjoint's segments (sinvb_rgf_checkpoints)
+    p.ckpt_every = e.ckpt ? max(1, (int)ceil(sqrt((double)e.n))) : 1;
     // small blocks keep FP64 DMMA products: the int8 path's fixed costs
     // (digit slicing, pipeline fill) outweigh its faster products there
     p.oz_digits = e.int8 ? oz_digits : 0;
@@ -411,7 +314,8 @@ static int launch_batched(void* ws, int count, unsigned flags, cudaStream_t stre
 template <class T>
 static int upload_and_run(const sinvb_batch_desc* d, int count, unsigned flags, void* ws, size_t ws_bytes,
                           int* status, cudaStream_t stream, int dtype, const unsigned* ready = nullptr,
-                          unsigned* done = nullptr, unsigned gen = 0, const sinvb_batch_schedule* sched = nullptr) {
+                          unsigned* done = nullptr, unsigned gen = 0, const sinvb_batch_schedule* sched = nullptr,
+                          void* const* ckpts = nullptr) {
   int rc = check_batch(d, count, flags, ws, ws_bytes, dtype, sched);
   if (rc) return rc;
   const BatchLayout L = batch_layout(d, count, dtype, flags, sched);
@@ -436,7 +340,7 @@ static int upload_and_run(const sinvb_batch_desc* d, int count, unsigned flags, 
     e.team = teams[k];
     e.slot_start = 0;
     e.int8 = mixed && d[k].b >= min_b;
-    e.pad[0] = e.pad[1] = 0;
+    e.ckpt = ckpts ? (T*)ckpts[k] : nullptr;
   }
   // longest first (by default cost ~ b^3 n; a schedule may give its own
   // estimates): long chains start while short ones fill in
@@ -558,6 +462,30 @@ int sinvb_rgf_batched_sched_d(const sinvb_batch_desc* descs, int count, unsigned
   if (flags & SINVB_PREC_MIXED) return SINVB_EUNSUPPORTED;
   return upload_and_run<double>(descs, count, flags, workspace, workspace_bytes, status, (cudaStream_t)stream,
                                 SINVB_F64, nullptr, nullptr, 0, sched);
+}
+
+int sinvb_rgf_batched_ckpt_z(const sinvb_batch_desc* descs, int count, unsigned flags, void* const* checkpoints,
+                             void* workspace, size_t workspace_bytes, int* status, sinvb_stream_t stream) {
+  if (!checkpoints || (flags & (SINVB_PREC_MIXED | SINVB_INPLACE))) return SINVB_EINVAL;
+  for (int k = 0; k < count; k++) {
+    if (!descs) return SINVB_EINVAL;
+    const int c = std::max(1, (int)std::ceil(std::sqrt((double)descs[k].n)));
+    if ((descs[k].n - 1) / c > 0 && (!checkpoints[k] || (uintptr_t)checkpoints[k] % 16)) return SINVB_EINVAL;
+  }
+  return upload_and_run<cplx>(descs, count, flags, workspace, workspace_bytes, status, (cudaStream_t)stream,
+                              SINVB_C128, nullptr, nullptr, 0, nullptr, checkpoints);
+}
+
+int sinvb_rgf_batched_ckpt_d(const sinvb_batch_desc* descs, int count, unsigned flags, void* const* checkpoints,
+                             void* workspace, size_t workspace_bytes, int* status, sinvb_stream_t stream) {
+  if (!checkpoints || (flags & (SINVB_PREC_MIXED | SINVB_INPLACE))) return SINVB_EINVAL;
+  for (int k = 0; k < count; k++) {
+    if (!descs) return SINVB_EINVAL;
+    const int c = std::max(1, (int)std::ceil(std::sqrt((double)descs[k].n)));
+    if ((descs[k].n - 1) / c > 0 && (!checkpoints[k] || (uintptr_t)checkpoints[k] % 8)) return SINVB_EINVAL;
+  }
+  return upload_and_run<double>(descs, count, flags, workspace, workspace_bytes, status, (cudaStream_t)stream,
+                                SINVB_F64, nullptr, nullptr, 0, nullptr, checkpoints);
 }
 
 int sinvb_rgf_batched_set_wait_limit(const void* workspace, double seconds) {

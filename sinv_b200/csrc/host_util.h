@@ -17,7 +17,7 @@ namespace sinvb {
     }                                               \
   } while (0)
 
-inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+__host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 // Records the last CUDA error seen by an entry point (per thread).
 void set_last_cuda_error(cudaError_t e);

@@ -81,12 +81,12 @@ def energy_loss_and_grad(H_onsite, H_coupling, energies, eta=1e-3, sigma=0.1, gr
     rank, world = rank_and_world(group)
     n, b = H_onsite.shape[0], H_onsite.shape[1]
     mine = shard_by_cost([1.0] * len(energies), world, rank)
-    if compute is None:
-        compute = _gpu_energy_term(H_onsite, H_coupling, eta, sigma)
     loss = torch.zeros((), dtype=torch.float64, device=H_onsite.device)
     g_on = torch.zeros_like(H_onsite, dtype=torch.float64)
     g_cp = torch.zeros_like(H_coupling, dtype=torch.float64)
-    for k in mine:
+    if compute is None and mine:  # this rank's energies as one batched forward and one batched adjoint
+        loss, g_on, g_cp = _gpu_energy_batch(H_onsite, H_coupling, [float(energies[k]) for k in mine], eta, sigma)
+    for k in (mine if compute is not None else []):
         l_k, go, gc = compute(float(energies[k]))
         loss += l_k
         g_on += go
@@ -98,6 +98,33 @@ def energy_loss_and_grad(H_onsite, H_coupling, energies, eta=1e-3, sigma=0.1, gr
         g_on = flat[1:1 + g_on.numel()].view_as(g_on)
         g_cp = flat[1 + g_on.numel():].view_as(g_cp)
     return loss, g_on, g_cp
+
+
+def _energy_matrix(Hd, Hu, E, eta, sigma):
+    """A(E) = (E + i eta) I - H - Sigma as block arrays (complex128), differentiable in H."""
+    import torch
+    b = Hd.shape[1]
+    eye = torch.eye(b, dtype=torch.complex128, device=Hd.device)
+    d = (E + 1j * eta) * eye - Hd.to(torch.complex128)
+    edge = torch.zeros_like(d)
+    edge[0] = 1j * sigma * eye
+    edge[-1] = edge[-1] + 1j * sigma * eye
+    return (d + edge, (-Hu.to(torch.complex128)).contiguous(),
+            (-Hu.transpose(1, 2).to(torch.complex128)).contiguous())
+
+
+def _gpu_energy_batch(H_onsite, H_coupling, energies, eta, sigma):
+    """Loss and dL/dH over `energies` with one batched forward launch and one
+    batched adjoint launch (the energy loop of the gradient as a batch)."""
+    import torch
+    from .algorithms.adjoint import rgf_batched_autograd
+    Hd = H_onsite.detach().clone().requires_grad_(True)
+    Hu = H_coupling.detach().clone().requires_grad_(True)
+    inst = [_energy_matrix(Hd, Hu, E, eta, sigma) for E in energies]
+    out = rgf_batched_autograd(inst)
+    loss = sum(-Gd.diagonal(0, 1, 2).imag.sum() / np.pi for (Gd, _, _) in out)
+    loss.backward()
+    return loss.detach(), Hd.grad.to(torch.float64), Hu.grad.to(torch.float64)
 
 
 def _gpu_energy_term(H_onsite, H_coupling, eta, sigma):
