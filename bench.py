@@ -270,6 +270,12 @@ def cpu_baseline(spec, reps=3):
 # cores (the library's cut-over; smaller blocks keep FP64 DMMA products).
 MIXED_MIN_B = 256
 INT8_PEAK_TOPS = 4500.0  # nominal dense int8 rate of a B200 (no measured figure on this pool)
+# DRAM bytes (read + write) per canonical flop of the batched kernel, from one
+# ncu capture of 37 instances of n = 8, b = 512 (profiles/rgf_batched_kernel_*.md):
+# 132.0 GB and 101.9 GB per launch for 2.54e12 canonical flops.  The operand
+# re-reads per output tile grow like b^3, as the flops do, so the launch's
+# traffic is estimated as this ratio times its canonical flops.
+TRAFFIC_BYTES_PER_FLOP = {"mixed": 132.0e9 / 2.54e12, "fp64": 101.9e9 / 2.54e12}
 
 
 def tensor_work(spec, precision, digits):
@@ -458,7 +464,11 @@ def run_sinvb(args, rank, world, local_rank):
                       "l2": "inputs larger than L2 in every wave", "parallelism": "replicas%d" % world},
            "gpu_launches": len(plans) * args.steps,
            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                        "frac": achieved / peak, "traffic": None,
+                        "frac": achieved / peak,
+                        "traffic": TRAFFIC_BYTES_PER_FLOP[args.precision] * sum(flops) / len(flops),
+                        "traffic_source": "ncu dram__bytes read+write of a 37-instance n=8 b=512 launch, "
+                                          "scaled to this launch by canonical flops",
+                        "algorithmic_bytes": sum(workloads.rgf_bytes(n, b) for (_, n, b, _) in spec) / len(flops),
                         "kernel": "rgf_batched_kernel", "flops": "canonical 8 b^3 (8(n-1)+n) per instance",
                         "frac_meaning": "FP64-equivalent: canonical flops per second over the FP64 DMMA peak; "
                                         "the tensor pipes actually used are in pipes",
