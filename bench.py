@@ -271,7 +271,7 @@ def cpu_baseline(spec, reps=3):
 MIXED_MIN_B = 256
 INT8_PEAK_TOPS = 4500.0  # nominal dense int8 rate of a B200 (no measured figure on this pool)
 # DRAM bytes (read + write) per canonical flop of the batched kernel, from one
-# ncu capture of 37 instances of n = 8, b = 512 (profiles/rgf_batched_kernel_*.md):
+# ncu capture of 37 instances of n = 8, b = 512 (one launch per precision):
 # 132.0 GB and 101.9 GB per launch for 2.54e12 canonical flops.  The operand
 # re-reads per output tile grow like b^3, as the flops do, so the launch's
 # traffic is estimated as this ratio times its canonical flops.

@@ -39,6 +39,20 @@ def _newest(paths):
     return max(os.path.getmtime(p) for p in paths)
 
 
+MAX_STACK_FRAME = 16384  # bytes per thread; the persistent kernels use 2-8 KB
+
+
+def stack_check(src, ptxas_log):
+    """Fails the build on a kernel whose stack size ptxas cannot determine
+    statically, or whose frame exceeds MAX_STACK_FRAME."""
+    import re
+    if "cannot be statically determined" in ptxas_log:
+        raise RuntimeError("%s: a kernel needs a dynamic stack (recursion):\n%s" % (src, ptxas_log))
+    frames = [int(x) for x in re.findall(r"(\d+) bytes stack frame", ptxas_log)]
+    if frames and max(frames) > MAX_STACK_FRAME:
+        raise RuntimeError("%s: stack frame of %d bytes exceeds %d" % (src, max(frames), MAX_STACK_FRAME))
+
+
 def build(force=False, verbose=False):
     """Compile every CUDA source and link the shared library.  Returns its path."""
     os.makedirs(BUILD, exist_ok=True)
@@ -46,7 +60,10 @@ def build(force=False, verbose=False):
     dep_time = _newest(_deps())
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= dep_time:
         return LIB
-    extra = ["-Xptxas", "-v"] if verbose else []
+    # ptxas reports every kernel's stack frame; stack_check refuses a kernel
+    # whose stack size it cannot determine statically (recursion), which would
+    # run with the per-thread stack limit instead of a frame sized at launch
+    extra = ["-Xptxas", "-v"]
 
     def compile_one(src):
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
@@ -56,6 +73,7 @@ def build(force=False, verbose=False):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("nvcc failed for %s:\n%s\n%s" % (src, r.stdout, r.stderr))
+        stack_check(src, r.stderr)
         return obj, r.stderr
 
     with ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
