@@ -325,10 +325,10 @@ def pipe_rates(spec, args, ms, dmma_peak):
 
 def run_reference(args, rank, world):
     """CPU reference arm: the reference RGF on the host cores.  A step is one
-    instance of the fixed stratified sample (cycling through it), timed on
-    the wall clock; ``ms_per_step`` is the median step actually timed.  The
-    matrices/s of the whole batch is extrapolated from the median seconds per
-    canonical flop of each block size over the timed steps."""
+    pass over the fixed stratified sample (the first PER_B instances of each
+    block size), timed on the wall clock; ``ms_per_step`` is the median pass.
+    The matrices/s of the whole batch is extrapolated from the median seconds
+    per canonical flop of each block size over the timed passes."""
     if rank != 0:
         return
     from oracle import rgf_oracle
@@ -336,38 +336,36 @@ def run_reference(args, rank, world):
     shape = tuple(int(x) for x in args.shape.split(",")) if args.shape else None
     spec = batch_spec(args.count, 0, shape)
     idx = cpu_sample(spec)
-    inst = {}
+    inst = {k: workloads.tight_binding(spec[k][1], spec[k][2], spec[k][0], seed=spec[k][3]) for k in idx}
     spf, steps_ms = {}, []
     for step in range(args.warmup + args.steps):
-        k = idx[step % len(idx)]
-        e, n, b, s = spec[k]
-        if k not in inst:
-            inst[k] = workloads.tight_binding(n, b, e, seed=s)
-        t0 = time.perf_counter()
-        rgf_oracle.rgf(*inst[k])
-        t = time.perf_counter() - t0
+        t_step = 0.0
+        for k in idx:
+            e, n, b, s = spec[k]
+            t0 = time.perf_counter()
+            rgf_oracle.rgf(*inst[k])
+            t = time.perf_counter() - t0
+            t_step += t
+            if step >= args.warmup:
+                spf.setdefault(b, []).append(t / workloads.rgf_flops(n, b))
         if step >= args.warmup:
-            steps_ms.append(1e3 * t)
-            spf.setdefault(b, []).append(t / workloads.rgf_flops(n, b))
-    # block sizes no timed step reached (very short runs) take the nearest timed rate by flops
-    for b in sorted({x[2] for x in spec}):
-        if b not in spf:
-            near = min(spf, key=lambda x: abs(x - b))
-            spf[b] = spf[near]
+            steps_ms.append(1e3 * t_step)
     spf_med = {b: statistics.median(v) for b, v in spf.items()}
     v = len(spec) / _extrapolate(spec, spf_med)
     env = _cpu_env()
+    sample = ", ".join("n=%d,b=%d" % (spec[k][1], spec[k][2]) for k in idx)
     cb = {"value": v, "unit": UNIT, "cores": env["blas_threads"], "kind": "port",
           "sample": "reference rgf (numpy/OpenBLAS restatement of rgf.py, the reference itself cannot run "
-                    "without its sources) on the fixed stratified sample (first %d instances of each block size), "
-                    "one instance per step, %d timed steps after %d warm-up steps; the batch's matrices/s "
-                    "extrapolated from the median seconds per canonical flop of each block size"
-                    % (PER_B, args.steps, args.warmup),
+                    "without its sources) on the fixed stratified sample (the first %d instances of each block "
+                    "size: %s), one pass over the sample per step, %d timed steps after %d warm-up steps; the "
+                    "batch's matrices/s extrapolated from the median seconds per canonical flop of each block size"
+                    % (PER_B, sample, args.steps, args.warmup),
           "extrapolated": True,
           "spread_seconds_per_flop": {str(b): [min(x), max(x)] for b, x in sorted(spf.items())}, **env}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(steps_ms),
-            "ms_per_step_meaning": "median wall time of one timed step (one sample instance), not of a batch",
+            "ms_per_step_meaning": "median wall time of one timed step: one pass over the %d-instance sample, "
+                                   "not over the batch" % len(idx),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
             "data": "synthetic", "config": {"workload": WORKLOAD, "count": args.count,
                                             "block_sizes": [64, 128, 256, 512], "n_range": [16, 128]},
@@ -705,12 +703,13 @@ def run_plain_large(args, rank, world, local_rank):
     is one selected inversion; every rank inverts its own copy (replicas)."""
     import torch
     from sinv_b200 import workloads
-    from sinv_b200.algorithms import bcr_s, psr_s, rgf, rgf2s
+    from sinv_b200.algorithms import bcr_s, pdiv_lm, psr_s, rgf, rgf2s
     from oracle import rgf_oracle
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     n, b = 64, 256
     psr_parts = [0, 3, 4, 8, 12]  # 0: the automatic choice
+    pdiv_parts = [2, 4, 8, 16]
     dn, un, ln = workloads.dominant(n, b, seed=0)
     d, u, l = (torch.from_numpy(x).to(dev) for x in (dn, un, ln))
     peak = dmma_peak_tflops(torch)
@@ -719,6 +718,7 @@ def run_plain_large(args, rank, world, local_rank):
     clocks = Clocks(local_rank) if rank == 0 else None
     ts, tb, t2 = [], [], []
     tp = {P: [] for P in psr_parts}
+    tq = {P: [] for P in pdiv_parts}
     for step in range(args.warmup + args.steps):
         if step == args.warmup and clocks:
             clocks.start()
@@ -732,9 +732,15 @@ def run_plain_large(args, rank, world, local_rank):
         for P in psr_parts:
             flush.zero_()
             mp[P] = _events_ms(torch, lambda: psr_s.psr_blocks(d, u, l, partitions=P or None, check=False), stream)
+        mq = {}
+        for P in pdiv_parts:
+            flush.zero_()
+            mq[P] = _events_ms(torch, lambda: pdiv_lm.pdiv_blocks(d, u, l, partitions=P, check=False), stream)
         if step >= args.warmup:
             for P in psr_parts:
                 tp[P].append(_max_over_ranks(torch, world, dev, mp[P]))
+            for P in pdiv_parts:
+                tq[P].append(_max_over_ranks(torch, world, dev, mq[P]))
             ts.append(_max_over_ranks(torch, world, dev, ms))
             tb.append(_max_over_ranks(torch, world, dev, mb))
             t2.append(_max_over_ranks(torch, world, dev, m2))
@@ -778,6 +784,10 @@ def run_plain_large(args, rank, world, local_rank):
                                         for P in psr_parts},
                    "rel_err_vs_oracle": max(float(np.linalg.norm(g.cpu().numpy() - r) / np.linalg.norm(r))
                                             for g, r in zip(psr_s.psr_blocks(d, u, l), R))},
+           "pdiv": {"ms_by_partitions": {str(P): statistics.median(tq[P]) for P in pdiv_parts},
+                    "rel_err_vs_oracle": {str(P): max(float(np.linalg.norm(g.cpu().numpy() - r) / np.linalg.norm(r))
+                                                      for g, r in zip(pdiv_lm.pdiv_blocks(d, u, l, partitions=P), R))
+                                          for P in pdiv_parts}},
            "clocks": clk,
            "e2e": {"value": world / (statistics.median(te) * 1e-3), "unit": "matrices/s",
                    "h2d_bytes_per_step": bytes_in, "d2h_bytes_per_step": bytes_in}}
@@ -994,8 +1004,8 @@ def run_gradient_set(args, rank, world, local_rank):
 
 def run_large_mixed(args, rank, world, local_rank):
     """Instances n=256, b=1024 (12.85 GB of input each), tight-binding generator,
-    mixed precision: 64 instances streamed through HBM in waves (as many as
-    fit in place, 13 on a B200); each wave's inputs are generated on the
+    mixed precision: 64 instances streamed through HBM in waves (equal waves of
+    at most what fits in place beside the workspace: 11 on a B200); each wave's inputs are generated on the
     device (untimed) and one persistent launch inverts the wave (timed).  A
     step is one pass over all instances.  The FP64 path runs the first wave
     once for comparison.  Error of the mixed path on a 4-block sub-instance
@@ -1011,7 +1021,10 @@ def run_large_mixed(args, rank, world, local_rank):
     peak = dmma_peak_tflops(torch)
     free, _ = torch.cuda.mem_get_info()
     per = in_elems(spec[0][1], spec[0][2])
-    wave = max(1, min(len(spec), int((free - 8e9) / 16) // per))
+    # headroom: the plan's workspace (scratch slots, digit planes) and the generator's temporaries
+    most = max(1, min(len(spec), int((free - 16e9) / 16) // per))
+    nwaves = -(-len(spec) // most)
+    wave = -(-len(spec) // nwaves)  # equal waves, the last one possibly shorter
     waves = [list(range(i, min(i + wave, len(spec)))) for i in range(0, len(spec), wave)]
     pool = torch.empty(wave * per, dtype=torch.complex128, device=dev)
     views = carve(pool, [spec[0]] * wave, list(range(wave)))
@@ -1020,6 +1033,8 @@ def run_large_mixed(args, rank, world, local_rank):
     def plan_for(w, precision):
         key = (len(w), precision)
         if key not in plans:
+            plans.clear()  # one plan (and workspace) at a time
+            torch.cuda.empty_cache()
             plans[key] = BatchPlan(views[:len(w)], precision=precision, inplace=True, digits=args.digits)
         return plans[key]
 

@@ -371,6 +371,27 @@ int sinvb_psr_part_d(const void* diag, const void* upper, const void* lower, int
                      int stage, void* boundary, void* G_diag, void* G_upper, void* G_lower, void* workspace,
                      size_t workspace_bytes, sinvb_stream_t stream);
 
+/* ---- PDIV: pairwise divide and conquer over partitions of one matrix ---------- */
+/*
+ * pdiv_localmap (src/sinv/algorithms/pdiv/pdiv_localmap.py:27-91) of all
+ * ``partitions`` processes at once: the block rows are split as
+ * pdiv_utils.py:84-123 does (n / P rows each, the remainder in the first);
+ * every partition's inverse, the log2(P) steps that merge neighbouring groups
+ * through the bridge blocks (twelve matrix maps and eight cross maps per
+ * partition) and the production of every partition's blocks and bridges run
+ * as one schedule on the whole GPU.  ``partitions`` must be a power of two,
+ * at most n and at most 64 (pdiv_utils.py:16-81), else SINVB_EINVAL.
+ * ``flags`` must be 0; the whole tridiagonal part of the inverse is written,
+ * the bridges between partitions included.
+ */
+size_t sinvb_pdiv_workspace_size(int n, int b, int partitions, int dtype, unsigned flags);
+int sinvb_pdiv_z(const void* diag, const void* upper, const void* lower, int n, int b, int partitions,
+                 unsigned flags, void* G_diag, void* G_upper, void* G_lower, void* workspace, size_t workspace_bytes,
+                 sinvb_stream_t stream);
+int sinvb_pdiv_d(const void* diag, const void* upper, const void* lower, int n, int b, int partitions,
+                 unsigned flags, void* G_diag, void* G_upper, void* G_lower, void* workspace, size_t workspace_bytes,
+                 sinvb_stream_t stream);
+
 /* ---- batched BCR: many independent matrices, levels in parallel -------------- */
 /*
  * bcr_serial (src/sinv/algorithms/bcr/bcr_serial.py:19-62) over a batch of

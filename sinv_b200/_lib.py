@@ -84,6 +84,9 @@ SIGNATURES = {
     "sinvb_psr_workspace_size": (_sz, [_i, _i, _i, _i, _u]),
     "sinvb_psr_z": (_i, [_vp, _vp, _vp, _i, _i, _i, _u, _vp, _vp, _vp, _vp, _sz, _vp]),
     "sinvb_psr_d": (_i, [_vp, _vp, _vp, _i, _i, _i, _u, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "sinvb_pdiv_workspace_size": (_sz, [_i, _i, _i, _i, _u]),
+    "sinvb_pdiv_z": (_i, [_vp, _vp, _vp, _i, _i, _i, _u, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "sinvb_pdiv_d": (_i, [_vp, _vp, _vp, _i, _i, _i, _u, _vp, _vp, _vp, _vp, _sz, _vp]),
     "sinvb_psr_part_workspace_size": (_sz, [_i, _i, _i, _i, _i]),
     "sinvb_psr_part_z": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "sinvb_psr_part_d": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
