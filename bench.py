@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--only", default=None, choices=["rgf", "bcr", "rgf2s", "psr", "pdiv"],
+                    help="plain_large: time only this algorithm (a short run for a profiler)")
     ap.add_argument("--tune", dest="tune", action="store_true", default=True,
                     help="teams, int8 cut-over and queue order from the autotuner (default)")
     ap.add_argument("--no-tune", dest="tune", action="store_false", help="the library's fixed rule instead")
@@ -297,13 +299,19 @@ def tensor_work(spec, precision, digits):
 
 
 # --------------------------------------------------------------------------- arms
-def schedule_summary(sched):
-    """The autotuner's choices for the bench line: teams used per block size,
-    the int8 cut-over and the estimate."""
+def schedule_summary(sched, shapes=None):
+    """The autotuner's choices for the bench line: the winning candidate, the
+    teams used per block size, the int8 cut-over and the estimate."""
     if not sched:
         return "fixed rule (teams by block size, int8 products from b=256)"
-    return {"int8_cutover_b": sched.get("int8_cutover"), "estimate_ms": round(sched["estimate_ms"], 1),
-            "teams_used": sorted({int(t) for t in sched["team"]})}
+    out = {"candidate": sched.get("candidate"), "int8_cutover_b": sched.get("int8_cutover"),
+           "estimate_ms": round(sched["estimate_ms"], 1), "teams_used": sorted({int(t) for t in sched["team"]})}
+    if shapes is not None and len(shapes) == len(sched["team"]):
+        by_b = {}
+        for (_, b), t in zip(shapes, sched["team"]):
+            by_b.setdefault(str(b), set()).add(int(t))
+        out["teams_by_b"] = {b: sorted(v) for b, v in sorted(by_b.items(), key=lambda kv: int(kv[0]))}
+    return out
 
 
 def pipe_rates(spec, args, ms, dmma_peak):
@@ -458,7 +466,7 @@ def run_sinvb(args, rank, world, local_rank):
            "config": {"workload": workload, "count": args.count, "block_sizes": [64, 128, 256, 512],
                       "n_range": [16, 128], "precision": args.precision, "path": "batched persistent",
                       "waves": len(waves), "wave_input_gb": round(pool_elems * 16 / 1e9, 2),
-                      "in_place": True, "schedule": schedule_summary(plans[0].schedule),
+                      "in_place": True, "schedule": schedule_summary(plans[0].schedule, [(spec[k][1], spec[k][2]) for k in waves[0]]),
                       "l2": "inputs larger than L2 in every wave", "parallelism": "replicas%d" % world},
            "gpu_launches": len(plans) * args.steps,
            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -719,6 +727,23 @@ def run_plain_large(args, rank, world, local_rank):
     ts, tb, t2 = [], [], []
     tp = {P: [] for P in psr_parts}
     tq = {P: [] for P in pdiv_parts}
+    if args.only:
+        calls = {"rgf": lambda: rgf.rgf_blocks(d, u, l, check=False),
+                 "bcr": lambda: bcr_s.bcr_blocks(d, u, l, check=False),
+                 "rgf2s": lambda: rgf2s.rgf2sided(d, u, l, check=False),
+                 "psr": lambda: psr_s.psr_blocks(d, u, l, partitions=4, check=False),
+                 "pdiv": lambda: pdiv_lm.pdiv_blocks(d, u, l, partitions=4, check=False)}
+        ts = []
+        for step in range(args.warmup + args.steps):
+            flush.zero_()
+            m = _events_ms(torch, calls[args.only], stream)
+            if step >= args.warmup:
+                ts.append(m)
+        return {"metric": "%s ms, one matrix n=64 b=256 (profiling run)" % args.only, "value": statistics.median(ts),
+                "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": statistics.median(ts), "higher_is_better": False,
+                "config": {"workload": "plain_large(n=64,b=256)", "only": args.only,
+                           "partitions": 4 if args.only in ("psr", "pdiv") else None}}
     for step in range(args.warmup + args.steps):
         if step == args.warmup and clocks:
             clocks.start()

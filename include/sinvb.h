@@ -454,8 +454,8 @@ int sinvb_fp64_mma_peak(int iters, double* tflops, sinvb_stream_t stream);
  * overlap an input or each other rejected (SINVB_EINVAL).  ``status``
  * (optional, device, one int) receives the device status.  The first call on
  * a device does its set-up (the array's address, the kernels' shared-memory
- * attributes): make it before any stream capture.  All calls share the
- * array, so calls that overlap on the GPU race.
+ * attributes).  All calls share the array, so calls that overlap on the GPU
+ * race.
  */
 int sinvb_rgf_z_noalloc(const void* diag, const void* upper, const void* lower, int n, int b,
                         unsigned flags, void* G_diag, void* G_upper, void* G_lower, int* status,

@@ -16,8 +16,7 @@
 //    the library holds it until the process exits;
 //  * the first call on a device does the set-up with that device current: it
 //    looks up the array's device address (cudaGetSymbolAddress) and sets the
-//    shared-memory attribute of both kernel instances; make that first call
-//    before any stream capture;
+//    shared-memory attribute of both kernel instances;
 //  * the output arrays must not overlap the inputs or each other (the sweep
 //    keeps per-row products in G_upper / G_lower while it still reads A);
 //    overlapping ranges are rejected with SINVB_EINVAL;

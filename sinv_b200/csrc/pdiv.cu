@@ -48,11 +48,11 @@ namespace {
 
 struct PdivPart {
   int s, m;  // first block row, block rows
-  size_t Kd, Ku, Kl, Cf, Cl, Rf, Rl, X, Pm, W, V, M[2], C, T, Y, Z, side;
+  size_t Kd, Ku, Kl, Cf, Cl, Rf, Rl, X, Pm, W, V, M[2], C, T, Y, Z, S, Xt, E, side;
 };
 
 struct PdivGroup {
-  size_t U, UY, J, Q, EH, side;
+  size_t U, UY, J, Jv, Jt, Je, I2, Q, EH, side;
 };
 
 struct PdivPlan {
@@ -110,6 +110,9 @@ PdivPlan pdiv_plan(int n, int b, int P) {
     q.T = take(6);
     q.Y = take(m + 2);
     q.Z = take(m + 2);
+    q.S = take(1);
+    q.Xt = take(1);
+    q.E = take(1);
     q.side = take_elems(invert_side_elems(b));
     L.parts.push_back(q);
   }
@@ -118,6 +121,10 @@ PdivPlan pdiv_plan(int n, int b, int P) {
     G.U = take(6);
     G.UY = take(4);
     G.J = take(4);
+    G.Jv = take(4);
+    G.Jt = take(4);
+    G.Je = take(4);
+    G.I2 = take(4);
     G.Q = take(4);
     G.EH = take(4);
     G.side = take_elems(invert_side_elems(2 * b));
@@ -160,15 +167,36 @@ void build_pdiv(Sched& s, const PdivPlan& L, const T* diag, const T* upper, cons
   int mmax = 0;
   for (const PdivPart& q : parts) mmax = std::max(mmax, q.m);
 
-  // ---- every partition's K blocks: forward sweep
-  s.begin();
+  // ---- every partition's K blocks: forward sweep.  Every block inverse
+  // gets one Newton step, X1 = X0 + X0 (I - S X0): a partition's first block
+  // is E - H_ii as given (no contact damping), whose leading sub-blocks can be
+  // ill conditioned, and the pivot-free blocked Gauss-Jordan loses digits on
+  // it that LAPACK's partial pivoting (the reference's inverse) keeps.
+  auto Sv = [&](int p) { return B(parts[p].S, 0); };
+  auto Xt = [&](int p) { return B(parts[p].Xt, 0); };
+  auto Ev = [&](int p) { return B(parts[p].E, 0); };
   std::vector<T*> inv, sides;
+  auto newton = [&](const std::vector<int>& ps, int row) {
+    inv.clear();
+    sides.clear();
+    for (int p : ps) {
+      inv.push_back(Xt(p));
+      sides.push_back(side(p));
+    }
+    invert_many<T>(s, inv, sides, b);
+    s.begin();
+    for (int p : ps) s.gemm(b, -1.0, Sv(p), Xt(p), I, Ev(p));  // E = I - S X0
+    s.begin();
+    for (int p : ps) s.gemm(b, 1.0, Xt(p), Ev(p), Xt(p), Kd(p, row));  // X1 = X0 + X0 E
+  };
+  s.begin();
+  std::vector<int> all;
   for (int p = 0; p < P; p++) {
-    s.copy(b, b, Ad(parts[p].s), b, Kd(p, 0), b);
-    inv.push_back(Kd(p, 0));
-    sides.push_back(side(p));
+    s.copy(b, b, Ad(parts[p].s), b, Sv(p), b);
+    s.copy(b, b, Ad(parts[p].s), b, Xt(p), b);
+    all.push_back(p);
   }
-  invert_many<T>(s, inv, sides, b);
+  newton(all, 0);
   for (int i = 0; i + 1 < mmax; i++) {
     s.begin();
     for (int p = 0; p < P; p++) {
@@ -178,18 +206,17 @@ void build_pdiv(Sched& s, const PdivPlan& L, const T* diag, const T* upper, cons
       s.gemm(b, 1.0, Al(r), Kd(p, i), nullptr, Pm(p, i));  // P_{i+1} = A_{i+1,i} g_i
     }
     s.begin();
-    inv.clear();
-    sides.clear();
+    std::vector<int> live;
     for (int p = 0; p < P; p++) {
       if (i + 1 >= parts[p].m) continue;
       const int r = parts[p].s + i;
-      s.gemm(b, -1.0, Pm(p, i), Au(r), Ad(r + 1), Kd(p, i + 1));           // S_{i+1}
+      s.gemm(b, -1.0, Pm(p, i), Au(r), Ad(r + 1), Sv(p));                      // S_{i+1}
+      s.gemm(b, -1.0, Pm(p, i), Au(r), Ad(r + 1), Xt(p));                      // (inverted in place)
       s.gemm(b, -1.0, Pm(p, i), i == 0 ? I : W(p, i), nullptr, W(p, i + 1));  // W_{i+1} = -P_{i+1} W_i
       s.gemm(b, -1.0, i == 0 ? I : V(p, i), X(p, i), nullptr, V(p, i + 1));   // V_{i+1} = -V_i X_i
-      inv.push_back(Kd(p, i + 1));
-      sides.push_back(side(p));
+      live.push_back(p);
     }
-    invert_many<T>(s, inv, sides, b);
+    newton(live, i + 1);
   }
   // ---- backward sweep, row i = m - 2 - t of every partition
   for (int t = 0; t + 1 < mmax; t++) {
@@ -267,25 +294,39 @@ void build_pdiv(Sched& s, const PdivPlan& L, const T* diag, const T* upper, cons
       s.gemm(b, 1.0, Cf(pm, lm), UY(G, 0), Kd(pm, lm), U(G, 2), Kd(pm, lm), UY(G, 1));
       s.gemm(b, 1.0, Kd(pn, 0), UY(G, 2), Kd(pn, 0), U(G, 3), Rf(pn, ln), UY(G, 3));
     }
-    // J = [[I, -U3 Bl], [-U2 Bu, I]]^{-1}, Bu / Bl the bridge after the middle process
+    // J = [[I, -U3 Bl], [-U2 Bu, I]]^{-1}, Bu / Bl the bridge after the middle
+    // process: assembled twice (Jt is inverted in place, Jv kept), one Newton
+    // step J = Jt + Jt (I - Jv Jt)
     s.begin();
     std::vector<T*> js, jside;
+    const size_t lo = (size_t)b * 2 * b;
     for (const Grp& G : grps) {
       const int r = parts[G.mid + 1].s - 1;
-      T* j = J(G);
-      s.copy(b, b, I, b, j, 2 * b);
-      s.copy(b, b, I, b, j + (size_t)b * 2 * b + b, 2 * b);
-      s.gemm(b, -1.0, U(G, 3), Al(r), nullptr, j + b, nullptr, nullptr, -1, b, b, b, b, b, 2 * b);
-      s.gemm(b, -1.0, U(G, 2), Au(r), nullptr, j + (size_t)b * 2 * b, nullptr, nullptr, -1, b, b, b, b, b, 2 * b);
-      js.push_back(j);
+      for (T* j : {base + G.g->Jt, base + G.g->Jv}) {
+        s.copy(b, b, I, b, j, 2 * b);
+        s.copy(b, b, I, b, j + lo + b, 2 * b);
+        s.gemm(b, -1.0, U(G, 3), Al(r), nullptr, j + b, nullptr, nullptr, -1, b, b, b, b, b, 2 * b);
+        s.gemm(b, -1.0, U(G, 2), Au(r), nullptr, j + lo, nullptr, nullptr, -1, b, b, b, b, b, 2 * b);
+      }
+      T* i2 = base + G.g->I2;
+      s.copy(b, b, I, b, i2, 2 * b);
+      s.copy(b, b, O, b, i2 + b, 2 * b);
+      s.copy(b, b, O, b, i2 + lo, 2 * b);
+      s.copy(b, b, I, b, i2 + lo + b, 2 * b);
+      js.push_back(base + G.g->Jt);
       jside.push_back(base + G.g->side);
     }
     invert_many<T>(s, js, jside, 2 * b);
     s.begin();
+    for (const Grp& G : grps)
+      s.gemm(2 * b, -1.0, base + G.g->Jv, base + G.g->Jt, base + G.g->I2, base + G.g->Je);
+    s.begin();
+    for (const Grp& G : grps)
+      s.gemm(2 * b, 1.0, base + G.g->Jt, base + G.g->Je, base + G.g->Jt, J(G));
+    s.begin();
     for (const Grp& G : grps) {
       const int r = parts[G.mid + 1].s - 1;
       T* j = J(G);
-      const size_t lo = (size_t)b * 2 * b;
       s.gemm(b, 1.0, Au(r), j, nullptr, Q(G, 0), nullptr, nullptr, -1, b, b, b, b, 2 * b, b);       // Bu J11
       s.gemm(b, 1.0, Au(r), j + b, nullptr, Q(G, 1), nullptr, nullptr, -1, b, b, b, b, 2 * b, b);   // Bu J12
       s.gemm(b, 1.0, Al(r), j + lo, nullptr, Q(G, 2), nullptr, nullptr, -1, b, b, b, b, 2 * b, b);  // Bl J21

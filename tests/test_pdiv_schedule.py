@@ -2,7 +2,8 @@
 
 ``sinv_b200/csrc/pdiv.cu`` does not form a partition's dense inverse K: it
 takes K's tridiagonal blocks and first / last block rows and columns from an
-RGF sweep pair (with the running products W_i, V_i), forms every group's
+RGF sweep pair (with the running products W_i, V_i; every block inverse and J
+with one Newton step), forms every group's
 shared factors once, splits each four-product map update into two products,
 and double-buffers the maps by reduction step.  ``schedule_mirror`` below
 restates that schedule op for op in numpy (same phases, same operands), and
@@ -21,6 +22,12 @@ from sinv_b200 import workloads
 from tests.golden.make_golden import PDIV_SIZES, PDIV_VARIANTS, banded_case
 
 
+def _newton_inv(S):
+    """Block inverse with the schedule's Newton step X1 = X0 + X0 (I - S X0)."""
+    X = np.linalg.inv(S)
+    return X + X @ (np.identity(S.shape[0], dtype=X.dtype) - S @ X)
+
+
 def schedule_mirror(diag, upper, lower, P):
     n, b = diag.shape[0], diag.shape[1]
     dt = np.result_type(diag, upper, lower)
@@ -37,7 +44,7 @@ def schedule_mirror(diag, upper, lower, P):
         parts.append(q)
     # forward sweeps
     for q in parts:
-        q["Kd"][0] = np.linalg.inv(diag[q["s"]])
+        q["Kd"][0] = _newton_inv(diag[q["s"]])
     for i in range(max(sizes) - 1):
         for q in parts:
             if i + 1 >= q["m"]:
@@ -52,7 +59,7 @@ def schedule_mirror(diag, upper, lower, P):
             S = diag[r + 1] - q["Pm"][i] @ upper[r]
             q["W"][i + 1] = -q["Pm"][i] @ (eye if i == 0 else q["W"][i])
             q["V"][i + 1] = -(eye if i == 0 else q["V"][i]) @ q["X"][i]
-            q["Kd"][i + 1] = np.linalg.inv(S)
+            q["Kd"][i + 1] = _newton_inv(S)
     # backward sweeps
     for t in range(max(sizes) - 1):
         for q in parts:
@@ -105,7 +112,7 @@ def schedule_mirror(diag, upper, lower, P):
             J[b:, b:] = eye
             J[:b, b:] = -U[3] @ Bl
             J[b:, :b] = -U[2] @ Bu
-            J = np.linalg.inv(J)
+            J = _newton_inv(J)
             Q = [Bu @ J[:b, :b], Bu @ J[:b, b:], Bl @ J[b:, :b], Bl @ J[b:, b:]]
             EH = [U[0] @ Q[1], U[5] @ Q[3], U[5] @ Q[2], U[0] @ Q[0]]
             for rr in range(start, end + 1):
