@@ -515,6 +515,12 @@ def run_sinvb(args, rank, world, local_rank):
     # accuracy of this precision against the FP64 path, on a sample of the batch
     if args.precision != "fp64":
         out["rel_err_vs_fp64"] = mixed_accuracy(torch, spec, args, dev)
+    # the reference's rgf run per matrix on the GPU through library calls
+    # (cuBLAS products, cuSOLVER inverses), on the CPU baseline's sample
+    if not args.no_plain:
+        lib = library_per_block(torch, spec, dev, stream)
+        lib["ratio"] = value / world / lib["matrices_per_s"]
+        out["vs_library_per_block_rgf"] = lib
     # e2e on a stratified sample (every 16th instance)
     if not args.no_e2e:
         try:
@@ -525,6 +531,46 @@ def run_sinvb(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(spec)
     return out
+
+
+def library_rgf(torch, d, u, l):
+    """The reference rgf (src/sinv/algorithms/rgf/rgf.py:40-64) with torch
+    operations on the GPU: one cuSOLVER inverse and cuBLAS complex products
+    per block, 8 products per block row as the reference writes them."""
+    n = d.shape[0]
+    inv, mm = torch.linalg.inv, torch.matmul
+    g = [None] * n
+    g[0] = inv(d[0])
+    for i in range(1, n):
+        g[i] = inv(d[i] - mm(mm(l[i - 1], g[i - 1]), u[i - 1]))
+    Gd, Gu, Gl = [None] * n, [None] * (n - 1), [None] * (n - 1)
+    Gd[n - 1] = g[n - 1]
+    for i in range(n - 2, -1, -1):
+        lf = mm(mm(Gd[i + 1], l[i]), g[i])
+        Gl[i] = -lf
+        Gu[i] = -mm(mm(g[i], u[i]), Gd[i + 1])
+        Gd[i] = g[i] + mm(mm(g[i], u[i]), lf)
+    return Gd, Gu, Gl
+
+
+def library_per_block(torch, spec, dev, stream):
+    """matrices/s of library_rgf over the batch: the fixed stratified sample
+    (two instances per block size), one untimed call then the median of 3
+    timed calls per instance (CUDA events), extrapolated to the batch by the
+    median seconds per canonical flop of each block size."""
+    from sinv_b200 import workloads
+    spf = {}
+    for k in cpu_sample(spec):
+        e, n, b, s = spec[k]
+        d, u, l = workloads.tight_binding_device(n, b, e, s, device=dev)
+        library_rgf(torch, d, u, l)
+        ts = [_events_ms(torch, lambda: library_rgf(torch, d, u, l), stream) for _ in range(3)]
+        spf.setdefault(b, []).append(statistics.median(ts) * 1e-3 / workloads.rgf_flops(n, b))
+        del d, u, l
+    med = {b: statistics.median(v) for b, v in spf.items()}
+    return {"matrices_per_s": len(spec) / _extrapolate(spec, med), "extrapolated": True,
+            "sample": "the reference rgf with torch ops on the GPU (cuSOLVER inverse, cuBLAS products, 8 products "
+                      "per block row), fixed stratified sample of 2 instances per block size, median of 3 calls each"}
 
 
 def plain_pass(torch, rgf, views, generate, stream):
