@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--wave-gb", type=float, default=0.0, help="input GB per wave (0: as much as HBM holds)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-per-b", type=int, default=PER_B,
+                    help="CPU sample: the first this many instances of each block size")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--only", default=None, choices=["rgf", "bcr", "rgf2s", "psr", "pdiv"],
                     help="plain_large: time only this algorithm (a short run for a profiler)")
@@ -203,8 +205,9 @@ def dmma_peak_tflops(torch):
 
 
 # The CPU baseline's fixed sample: the first PER_B instances of each block
-# size in the batch's order (same seeds and energies as the GPU run).
-PER_B = 2
+# size in the batch's order (same seeds and energies as the GPU run), 32
+# instances of the 512.
+PER_B = 8
 
 
 def cpu_sample(spec, per_b=PER_B):
@@ -230,7 +233,7 @@ def _extrapolate(spec, spf_by_b):
     return sum(workloads.rgf_flops(n, b) * spf_by_b[b] for (_, n, b, _) in spec)
 
 
-def cpu_baseline(spec, reps=3):
+def cpu_baseline(spec, reps=3, per_b=PER_B):
     """The reference RGF (numpy restatement of src/sinv/algorithms/rgf/rgf.py,
     the same numpy / OpenBLAS calls in the same order) on the host cores: the
     fixed stratified sample (two instances per block size), each timed
@@ -239,7 +242,7 @@ def cpu_baseline(spec, reps=3):
     block size (marked as extrapolated)."""
     from oracle import rgf_oracle
     from sinv_b200 import workloads
-    idx = cpu_sample(spec)
+    idx = cpu_sample(spec, per_b)
     spf = {}
     timed, sampled = 0.0, []
     warm = workloads.tight_binding(*spec[idx[0]][1:3], spec[idx[0]][0], seed=spec[idx[0]][3])
@@ -263,7 +266,7 @@ def cpu_baseline(spec, reps=3):
             "sample": "reference rgf (numpy/OpenBLAS restatement) on a fixed stratified sample (the first %d "
                       "instances of each block size: %s), median of %d timed runs each after a warm-up; "
                       "batch time extrapolated from the median seconds per canonical flop of each block size"
-                      % (PER_B, ", ".join(sampled), reps),
+                      % (per_b, ", ".join(sampled), reps),
             "extrapolated": True, "timed_seconds": timed,
             "spread_seconds_per_flop": {str(b): [min(v), max(v)] for b, v in sorted(spf.items())}, **env}
 
@@ -343,7 +346,7 @@ def run_reference(args, rank, world):
     from sinv_b200 import workloads
     shape = tuple(int(x) for x in args.shape.split(",")) if args.shape else None
     spec = batch_spec(args.count, 0, shape)
-    idx = cpu_sample(spec)
+    idx = cpu_sample(spec, args.cpu_per_b)
     inst = {k: workloads.tight_binding(spec[k][1], spec[k][2], spec[k][0], seed=spec[k][3]) for k in idx}
     spf, steps_ms = {}, []
     for step in range(args.warmup + args.steps):
@@ -367,7 +370,7 @@ def run_reference(args, rank, world):
                     "without its sources) on the fixed stratified sample (the first %d instances of each block "
                     "size: %s), one pass over the sample per step, %d timed steps after %d warm-up steps; the "
                     "batch's matrices/s extrapolated from the median seconds per canonical flop of each block size"
-                    % (PER_B, sample, args.steps, args.warmup),
+                    % (args.cpu_per_b, sample, args.steps, args.warmup),
           "extrapolated": True,
           "spread_seconds_per_flop": {str(b): [min(x), max(x)] for b, x in sorted(spf.items())}, **env}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
@@ -529,7 +532,7 @@ def run_sinvb(args, rank, world, local_rank):
             out["e2e"] = e2e_sample(torch, spec, args, dev, world)
             out["e2e"]["streamed_unavailable"] = str(err)[:200]
     if rank == 0 and world == 1 and not args.no_cpu:
-        out["cpu_baseline"] = cpu_baseline(spec)
+        out["cpu_baseline"] = cpu_baseline(spec, per_b=args.cpu_per_b)
     return out
 
 
@@ -560,7 +563,7 @@ def library_per_block(torch, spec, dev, stream):
     median seconds per canonical flop of each block size."""
     from sinv_b200 import workloads
     spf = {}
-    for k in cpu_sample(spec):
+    for k in cpu_sample(spec, per_b=2):
         e, n, b, s = spec[k]
         d, u, l = workloads.tight_binding_device(n, b, e, s, device=dev)
         library_rgf(torch, d, u, l)
