@@ -283,7 +283,7 @@ INT8_PEAK_TOPS = 4500.0  # nominal dense int8 rate of a B200 (no measured figure
 TRAFFIC_BYTES_PER_FLOP = {"mixed": 132.0e9 / 2.54e12, "fp64": 101.9e9 / 2.54e12}
 
 
-def tensor_work(spec, precision, digits):
+def tensor_work(spec, precision, digits, mixed_min_b=None):
     """Work the batched schedule issues per pass, by pipe: int8 tensor-core ops
     of the Ozaki products (S(S+1)/2 digit pairs, each a real (2b) x b x (2b)
     product, 2 ops per multiply-add; 6 (n-1) products per instance), and FP64
@@ -291,10 +291,11 @@ def tensor_work(spec, precision, digits):
     products of blocks the mixed path leaves in FP64)."""
     int8, fp64 = 0.0, 0.0
     pairs = digits * (digits + 1) // 2
+    cut = MIXED_MIN_B if mixed_min_b is None else mixed_min_b
     for (_, n, b, _) in spec:
         prods = 6 * (n - 1)
         fp64 += 8.0 * n * b ** 3
-        if precision == "mixed" and b >= MIXED_MIN_B:
+        if precision == "mixed" and b >= cut:
             int8 += prods * pairs * 2.0 * (2 * b) * b * (2 * b)
         else:
             fp64 += prods * 8.0 * b ** 3
@@ -317,12 +318,13 @@ def schedule_summary(sched, shapes=None):
     return out
 
 
-def pipe_rates(spec, args, ms, dmma_peak):
+def pipe_rates(spec, args, ms, dmma_peak, mixed_min_b=None):
     """Average rates of the two tensor pipes over one pass (counted work /
-    device time of the pass)."""
+    device time of the pass); ``mixed_min_b``: the smallest block size whose
+    products ran on the int8 pipe (the schedule's cut-over)."""
     if ms <= 0:
         return None
-    int8, fp64 = tensor_work(spec, args.precision, args.digits)
+    int8, fp64 = tensor_work(spec, args.precision, args.digits, mixed_min_b)
     sec = ms * 1e-3
     out = {"dmma": {"tflops": fp64 / sec / 1e12, "frac_of_dmma_peak": fp64 / sec / 1e12 / dmma_peak,
                     "work": "every block inverse (b^3 complex multiply-adds) and the products left in FP64"}}
@@ -484,7 +486,8 @@ def run_sinvb(args, rank, world, local_rank):
                         "peak_source": "FP64 tensor-core (DMMA) rate measured at start on this GPU by "
                                        "sinvb_fp64_mma_peak (MEASURED_PEAKS.json has no FP64 figure)",
                         "peak_dgemm_cublas": dgemm_peak,
-                        "pipes": pipe_rates(spec, args, sum(kern_ms) / max(1, args.steps), peak)},
+                        "pipes": pipe_rates(spec, args, sum(kern_ms) / max(1, args.steps), peak,
+                                             (plans[0].schedule or {}).get("mixed_min_b"))},
            "clocks": clk}
 
     # the plain per-matrix FP64 path (one library call per instance, the whole
