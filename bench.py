@@ -303,9 +303,11 @@ def tensor_work(spec, precision, digits, mixed_min_b=None):
 
 
 # --------------------------------------------------------------------------- arms
-def schedule_summary(sched, shapes=None):
+def schedule_summary(sched, shapes=None, table=None):
     """The autotuner's choices for the bench line: the winning candidate, the
-    teams used per block size, the int8 cut-over and the estimate."""
+    teams used per block size, the int8 cut-over and the estimate, and the
+    measured block-row latency (ms, GPU full) of every (block size, team,
+    product path) it chose from."""
     if not sched:
         return "fixed rule (teams by block size, int8 products from b=256)"
     out = {"candidate": sched.get("candidate"), "int8_cutover_b": sched.get("int8_cutover"),
@@ -315,6 +317,9 @@ def schedule_summary(sched, shapes=None):
         for (_, b), t in zip(shapes, sched["team"]):
             by_b.setdefault(str(b), set()).add(int(t))
         out["teams_by_b"] = {b: sorted(v) for b, v in sorted(by_b.items(), key=lambda kv: int(kv[0]))}
+    if table:
+        out["row_ms"] = {b: {t: {path: round(c["row_ms"], 3) for path, c in paths.items()}
+                             for t, paths in teams.items()} for b, teams in table.items()}
     return out
 
 
@@ -400,10 +405,13 @@ def run_sinvb(args, rank, world, local_rank):
     dgemm_peak = fp64_peak_tflops(torch)
     peak = dmma_peak_tflops(torch)
 
+    tune_table = None
     if args.tune:  # measure (or load) the autotuner's table before the input pool takes HBM
         from sinv_b200 import autotune
         for prec in {args.precision, "fp64"}:
-            autotune.load_or_measure(sorted({b for (_, _, b, _) in spec}), prec, args.digits, dev)
+            tab = autotune.load_or_measure(sorted({b for (_, _, b, _) in spec}), prec, args.digits, dev)
+            if prec == args.precision:
+                tune_table = tab
         torch.cuda.empty_cache()
     free, _ = torch.cuda.mem_get_info()
     # In place (results over the inputs): the whole batch fits in HBM as one
@@ -471,7 +479,8 @@ def run_sinvb(args, rank, world, local_rank):
            "config": {"workload": workload, "count": args.count, "block_sizes": [64, 128, 256, 512],
                       "n_range": [16, 128], "precision": args.precision, "path": "batched persistent",
                       "waves": len(waves), "wave_input_gb": round(pool_elems * 16 / 1e9, 2),
-                      "in_place": True, "schedule": schedule_summary(plans[0].schedule, [(spec[k][1], spec[k][2]) for k in waves[0]]),
+                      "in_place": True, "schedule": schedule_summary(plans[0].schedule, [(spec[k][1], spec[k][2]) for k in waves[0]],
+                                                   tune_table),
                       "l2": "inputs larger than L2 in every wave", "parallelism": "replicas%d" % world},
            "gpu_launches": len(plans) * args.steps,
            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
