@@ -670,7 +670,8 @@ def e2e_streamed(torch, spec, args, dev, world):
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        rgf_batched_host(host, outputs=host, precision=args.precision, digits=args.digits, device=dev)
+        rgf_batched_host(host, outputs=host, precision=args.precision, digits=args.digits, device=dev,
+                         schedule="tune" if args.tune else None)
         t = time.perf_counter() - t0
         if world > 1:
             tt = torch.tensor([t], dtype=torch.float64, device=dev)
@@ -687,8 +688,10 @@ def e2e_streamed(torch, spec, args, dev, world):
             "h2d_bytes_per_step": bytes_step, "d2h_bytes_per_step": bytes_step,
             "sample": ("the whole batch" if len(idx) == len(spec) else
                        "every %dth instance (%d)" % (len(spec) // len(idx), len(idx)))
-                      + ", %.0f GB each way through pinned host memory; rgf_batched_host (%s) overlaps the "
-                        "copies with the sweeps; wall clock around the call" % (bytes_step / 1e9, mode)}
+                      + ", %.0f GB each way through pinned host memory; rgf_batched_host (%s%s) overlaps the "
+                        "copies with the sweeps; wall clock around the call"
+                      % (bytes_step / 1e9, mode, ", teams and queue order from autotune.stream_schedule"
+                         if args.tune else "")}
 
 
 def e2e_sample(torch, spec, args, dev, world):

@@ -265,6 +265,17 @@ int sinvb_rgf_batched_sched_z(const sinvb_batch_desc* descs, int count, unsigned
 int sinvb_rgf_batched_sched_d(const sinvb_batch_desc* descs, int count, unsigned flags,
                               const sinvb_batch_schedule* sched, void* workspace, size_t workspace_bytes,
                               int* status, sinvb_stream_t stream);
+/* sinvb_rgf_batched_stream_z / _d with a schedule (NULL: as without).  The
+ * queue takes the instances in descending priority, ties in descriptor order;
+ * the caller copies them in that order. */
+int sinvb_rgf_batched_stream_sched_z(const sinvb_batch_desc* descs, int count, unsigned flags,
+                                     const sinvb_batch_schedule* sched, void* workspace, size_t workspace_bytes,
+                                     int* status, const unsigned* ready, unsigned* done, unsigned gen,
+                                     sinvb_stream_t stream);
+int sinvb_rgf_batched_stream_sched_d(const sinvb_batch_desc* descs, int count, unsigned flags,
+                                     const sinvb_batch_schedule* sched, void* workspace, size_t workspace_bytes,
+                                     int* status, const unsigned* ready, unsigned* done, unsigned gen,
+                                     sinvb_stream_t stream);
 
 /*
  * Batched forward sweeps that also save the adjoint's checkpoints (the

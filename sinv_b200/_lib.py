@@ -55,6 +55,8 @@ SIGNATURES = {
     "sinvb_rgf_batched_d": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp]),
     "sinvb_rgf_batched_stream_z": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp, _vp, _u, _vp]),
     "sinvb_rgf_batched_stream_d": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp, _vp, _u, _vp]),
+    "sinvb_rgf_batched_stream_sched_z": (_i, [_vp, _i, _u, _vp, _vp, _sz, _vp, _vp, _vp, _u, _vp]),
+    "sinvb_rgf_batched_stream_sched_d": (_i, [_vp, _i, _u, _vp, _vp, _sz, _vp, _vp, _vp, _u, _vp]),
     "sinvb_rgf_batched_rerun_z": (_i, [_vp, _vp]),
     "sinvb_rgf_batched_rerun_d": (_i, [_vp, _vp]),
     "sinvb_rgf_batched_set_wait_limit": (_i, [_vp, ctypes.c_double]),

@@ -229,12 +229,31 @@ class BatchPlan:
         descriptors again on every call."""
         torch = dev._torch()
         with torch.cuda.device(self.device):
-            fn = self.lib.sinvb_rgf_batched_stream_z if self.code == _lib.C128 else self.lib.sinvb_rgf_batched_stream_d
-            rc = fn(ctypes.cast(self.descs, ctypes.c_void_p), len(self.descs), self.flags, dev.ptr(self.ws),
-                    self.ws.numel(), dev.ptr(self.status_dev), dev.ptr(ready), dev.ptr(done), int(gen),
-                    dev.stream_handle(stream))
+            if self._sched is not None:
+                fn = (self.lib.sinvb_rgf_batched_stream_sched_z if self.code == _lib.C128
+                      else self.lib.sinvb_rgf_batched_stream_sched_d)
+                rc = fn(ctypes.cast(self.descs, ctypes.c_void_p), len(self.descs), self.flags, self._sched_ptr(),
+                        dev.ptr(self.ws), self.ws.numel(), dev.ptr(self.status_dev), dev.ptr(ready), dev.ptr(done),
+                        int(gen), dev.stream_handle(stream))
+            else:
+                fn = (self.lib.sinvb_rgf_batched_stream_z if self.code == _lib.C128
+                      else self.lib.sinvb_rgf_batched_stream_d)
+                rc = fn(ctypes.cast(self.descs, ctypes.c_void_p), len(self.descs), self.flags, dev.ptr(self.ws),
+                        self.ws.numel(), dev.ptr(self.status_dev), dev.ptr(ready), dev.ptr(done), int(gen),
+                        dev.stream_handle(stream))
             _lib.check(rc, "sinvb_rgf_batched_stream")
             self.uploaded = True
+
+    def queue_order(self):
+        """Instance indices in the order the kernel's queue hands them out:
+        descending priority (the schedule's, as float32, else b^3 n), ties in
+        instance order.  A streamed run copies its inputs in this order."""
+        pr = (self.schedule or {}).get("priority") if isinstance(self.schedule, dict) else None
+        if pr is not None:
+            key = [float(np.float32(p)) for p in pr]
+        else:
+            key = [float(b) ** 3 * n for n, b in self.shapes]
+        return sorted(range(len(self.shapes)), key=lambda k: -key[k])
 
     def statuses(self):
         """Per-instance device status (synchronises)."""
@@ -287,7 +306,7 @@ def _available_bytes(torch, device):
 
 
 def rgf_batched_host(instances, outputs=None, sym_mat=False, precision="fp64", digits=7, wave_bytes=None,
-                     device=None, check=True):
+                     device=None, check=True, schedule=None):
     """Selected inversion of host-resident instances streamed through the GPU.
 
     ``instances``: list of ``(A_diag, A_upper, A_lower)`` torch CPU tensors
@@ -301,7 +320,11 @@ def rgf_batched_host(instances, outputs=None, sym_mat=False, precision="fp64", d
     one persistent launch, in place in one of two device buffers, while the
     next wave's inputs copy in on one stream and the previous wave's results
     copy out on another, so PCIe traffic hides behind the sweeps.  Off-diagonal
-    blocks are always computed.
+    blocks are always computed.  ``schedule`` (when the batch fits as one
+    launch): teams and queue order as for ``BatchPlan``, or ``"tune"`` for the
+    autotuner's choice for a streamed batch (``autotune.stream_schedule``,
+    from the measured table of this GPU); the inputs are copied in the
+    queue's order.
     """
     torch = dev._torch()
     device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -313,7 +336,8 @@ def rgf_batched_host(instances, outputs=None, sym_mat=False, precision="fp64", d
         esize_ = 16 if tdt == torch.complex128 else 8
         total = sum((3 * int(d.shape[0]) - 2) * int(d.shape[1]) ** 2 for d, _, _ in instances) * esize_
         if total + (8 << 30) <= free:  # the whole batch fits: one launch, copies overlapping it
-            return _host_one_launch(torch, instances, outputs, sym_mat, precision, digits, device, check)
+            return _host_one_launch(torch, instances, outputs, sym_mat, precision, digits, device, check,
+                                    schedule)
     if tdt not in (torch.complex128, torch.float64):
         raise TypeError("rgf_batched_host takes complex128 or float64 host tensors")
     shapes = [(int(d.shape[0]), int(d.shape[1])) for d, _, _ in instances]
@@ -387,7 +411,7 @@ def rgf_batched_host(instances, outputs=None, sym_mat=False, precision="fp64", d
 _gen_counter = [0]
 
 
-def _host_one_launch(torch, instances, outputs, sym_mat, precision, digits, device, check):
+def _host_one_launch(torch, instances, outputs, sym_mat, precision, digits, device, check, schedule=None):
     """rgf_batched_host when the whole batch fits on the device: one persistent
     launch whose teams wait for each instance's inputs (ready flags written
     after its copies) while the host copies them in, largest b^3 n first (the
@@ -397,7 +421,13 @@ def _host_one_launch(torch, instances, outputs, sym_mat, precision, digits, devi
     shapes = [(int(d.shape[0]), int(d.shape[1])) for d, _, _ in instances]
     if outputs is None:
         outputs = [(torch.empty_like(d), torch.empty_like(u), torch.empty_like(l)) for d, u, l in instances]
-    order = sorted(range(len(shapes)), key=lambda k: -(shapes[k][1] ** 3) * shapes[k][0])  # stable, as the kernel
+    if isinstance(schedule, str):
+        if schedule != "tune":
+            raise ValueError("schedule must be a dict, None or 'tune'")
+        from .. import autotune
+        table = autotune.load_or_measure(sorted({b for _, b in shapes}), precision, int(digits), device)
+        sms = torch.cuda.get_device_properties(device).multi_processor_count
+        schedule = autotune.stream_schedule(shapes, table, sms, precision, 16 if tdt == torch.complex128 else 8)
     _gen_counter[0] += 1
     gen = _gen_counter[0]
     with torch.cuda.device(device):
@@ -420,7 +450,9 @@ def _host_one_launch(torch, instances, outputs, sym_mat, precision, digits, devi
         for s_ in (s_in, s_run, s_out, s_poll):
             s_.wait_event(init)
         with torch.cuda.stream(s_run):
-            plan = BatchPlan(views, sym_mat=sym_mat, precision=precision, inplace=True, digits=digits)
+            plan = BatchPlan(views, sym_mat=sym_mat, precision=precision, inplace=True, digits=digits,
+                             schedule=schedule)
+        order = plan.queue_order()  # copy the inputs in the order the kernel's teams take them
         plan.run_streamed(ready, done, gen, s_run)
         with torch.cuda.stream(s_in):
             for k in order:

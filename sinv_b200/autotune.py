@@ -290,3 +290,71 @@ def schedule(shapes, table, sms, precision="mixed"):
             "mixed_min_b": (int(cut) if cut is not None else never) if precision == "mixed" else 0,
             "int8_cutover": cut, "estimate_ms": span, "work_ms": work(team), "chain_ms": max(durs),
             "candidate": name}
+
+
+def simulate_stream(durations, teams, order, in_bytes, sms, h2d_gbs=55.0, d2h_gbs=55.0):
+    """Wall time (ms) of a host-streamed batch (rgf_batched_host, one launch):
+    inputs copied in queue order at ``h2d_gbs``; an instance starts when its
+    inputs have arrived and its team's members are free (members handed to
+    the first free CTAs, as ``simulate``); results copied out one after
+    another at ``d2h_gbs`` in the order instances finish.  ``in_bytes``: the
+    input (= output) bytes of each instance."""
+    import heapq
+    free = [(0.0, c) for c in range(sms)]
+    heapq.heapify(free)
+    arrive, t = {}, 0.0
+    for k in order:
+        t += in_bytes[k] / (h2d_gbs * 1e6)
+        arrive[k] = t
+    finish = []
+    for k in order:
+        members = [heapq.heappop(free) for _ in range(min(teams[k], sms))]
+        start = max([arrive[k]] + [f for f, _ in members])
+        end = start + durations[k]
+        finish.append((end, k))
+        for _, c in members:
+            heapq.heappush(free, (end, c))
+    out = 0.0
+    for end, k in sorted(finish):
+        out = max(out, end) + in_bytes[k] / (d2h_gbs * 1e6)
+    return out
+
+
+def stream_schedule(shapes, table, sms, precision="mixed", elem_bytes=16, h2d_gbs=55.0, d2h_gbs=55.0):
+    """Teams and queue order for a host-streamed batch: the candidates of
+    ``schedule`` plus every instance on its fastest team (shortest chain) and
+    that for the largest block size only, each queued longest first, judged
+    by ``simulate_stream`` (copy-in, sweeps and copy-out overlapped).  Copies
+    make late finishers expensive: an instance that ends after the last input
+    has arrived still has its results to copy out, so shorter chains can win
+    over the device-resident makespan choice.  Returns the ``schedule`` dict
+    with "estimate_ms" the simulated wall time."""
+    base = schedule(shapes, table, sms, precision)
+    mixed_min_b = base["mixed_min_b"]
+
+    def costs(b, t):
+        row = table[_nearest(table, b)]
+        key = str(t) if str(t) in row else min(row, key=lambda x: abs(int(x) - t))
+        c = row[key]
+        path = "int8" if (precision == "mixed" and b >= mixed_min_b and "int8" in c) else "fp64"
+        return c[path]
+
+    rows = [(n - 1) if n > 1 else 1 for n, _ in shapes]
+    in_bytes = [(3 * n - 2) * b * b * elem_bytes for n, b in shapes]
+    choices = [sorted(t for t in (int(x) for x in table[_nearest(table, b)]) if t <= sms) for _, b in shapes]
+    fastest = [min(ts, key=lambda t: costs(b, t)["row_ms"]) for ts, (_, b) in zip(choices, shapes)]
+    bmax = max(b for _, b in shapes)
+    cands = {"tuned " + base["candidate"]: base["team"], "fixed rule": fixed_rule_teams(shapes, sms),
+             "fastest": fastest,
+             "fastest for b=%d" % bmax: [f if b == bmax else t for f, t, (_, b) in zip(fastest, base["team"], shapes)]}
+    best = None
+    for name, team in cands.items():
+        d = [r * costs(b, t)["row_ms"] for r, (_, b), t in zip(rows, shapes, team)]
+        order = sorted(range(len(shapes)), key=lambda k: -d[k])
+        wall = simulate_stream(d, team, order, in_bytes, sms, h2d_gbs, d2h_gbs)
+        if best is None or wall < best[0]:
+            best = (wall, name, team, d)
+    wall, name, team, d = best
+    out = dict(base)
+    out.update({"team": team, "priority": d, "estimate_ms": wall, "candidate": name, "chain_ms": max(d)})
+    return out

@@ -464,6 +464,29 @@ int sinvb_rgf_batched_sched_d(const sinvb_batch_desc* descs, int count, unsigned
                                 SINVB_F64, nullptr, nullptr, 0, sched);
 }
 
+int sinvb_rgf_batched_stream_sched_z(const sinvb_batch_desc* descs, int count, unsigned flags,
+                                     const sinvb_batch_schedule* sched, void* workspace, size_t workspace_bytes,
+                                     int* status, const unsigned* ready, unsigned* done, unsigned gen,
+                                     sinvb_stream_t stream) {
+  if (!ready || !done || gen == 0) return SINVB_EINVAL;
+  if ((flags & SINVB_PREC_MIXED) && mixed_digits(flags) > kOzMaxDigits) return SINVB_EINVAL;
+  if (flags & SINVB_PREC_MIXED)
+    for (int k = 0; k < count; k++)
+      if (descs && descs[k].b >= mixed_min_b(sched) && 2 * descs[k].b > (1 << 14)) return SINVB_EINVAL;
+  return upload_and_run<cplx>(descs, count, flags, workspace, workspace_bytes, status, (cudaStream_t)stream,
+                              SINVB_C128, ready, done, gen, sched);
+}
+
+int sinvb_rgf_batched_stream_sched_d(const sinvb_batch_desc* descs, int count, unsigned flags,
+                                     const sinvb_batch_schedule* sched, void* workspace, size_t workspace_bytes,
+                                     int* status, const unsigned* ready, unsigned* done, unsigned gen,
+                                     sinvb_stream_t stream) {
+  if (!ready || !done || gen == 0) return SINVB_EINVAL;
+  if (flags & SINVB_PREC_MIXED) return SINVB_EUNSUPPORTED;
+  return upload_and_run<double>(descs, count, flags, workspace, workspace_bytes, status, (cudaStream_t)stream,
+                                SINVB_F64, ready, done, gen, sched);
+}
+
 int sinvb_rgf_batched_ckpt_z(const sinvb_batch_desc* descs, int count, unsigned flags, void* const* checkpoints,
                              void* workspace, size_t workspace_bytes, int* status, sinvb_stream_t stream) {
   if (!checkpoints || (flags & (SINVB_PREC_MIXED | SINVB_INPLACE))) return SINVB_EINVAL;

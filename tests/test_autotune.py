@@ -98,3 +98,36 @@ def test_schedule_never_worse_than_fixed_rule_in_simulation():
         return out
     d = dur(fixed)
     assert s["estimate_ms"] <= autotune.simulate(d, fixed, d, 16) + 1e-9
+
+
+def test_simulate_stream_one_instance():
+    # 1 GB in at 10 GB/s (100 ms), 50 ms of sweeps, 1 GB out (100 ms)
+    wall = autotune.simulate_stream([50.0], [1], [0], [1e9], 4, h2d_gbs=10.0, d2h_gbs=10.0)
+    assert abs(wall - 250.0) < 1e-9
+
+
+def test_simulate_stream_overlaps_copies():
+    # two instances on two CTAs: the second copy-in overlaps the first sweep,
+    # the first copy-out overlaps the second sweep
+    wall = autotune.simulate_stream([100.0, 100.0], [1, 1], [0, 1], [1e9, 1e9], 2, h2d_gbs=10.0, d2h_gbs=10.0)
+    assert abs(wall - 400.0) < 1e-9   # in 0-100, 100-200; sweeps 100-200, 200-300; out 200-300, 300-400
+
+
+def test_stream_schedule_prefers_short_chains_when_copies_dominate():
+    # b = 512: team 8 halves the chain at a 30 % SM-time premium; with the
+    # copies in the way, the streamed choice takes the short chains while the
+    # device-resident makespan choice keeps the cheaper teams
+    tab = {"512": {"2": {"fp64": {"row_ms": 16.0, "sm_ms": 32.0}}, "4": {"fp64": {"row_ms": 8.5, "sm_ms": 34.0}},
+                   "8": {"fp64": {"row_ms": 5.2, "sm_ms": 41.6}}},
+           "64": {"1": {"fp64": {"row_ms": 0.05, "sm_ms": 0.05}}}}
+    shapes = [(100, 512)] * 40 + [(60, 64)] * 200
+    s = autotune.stream_schedule(shapes, tab, 148, "fp64")
+    assert len(s["team"]) == len(shapes) and len(s["priority"]) == len(shapes)
+    assert all(t in (1, 2, 4, 8) for t in s["team"])
+    walls = {}
+    for name, team in (("cheap", [2] * 40 + [1] * 200), ("short", [8] * 40 + [1] * 200)):
+        d = [99 * (16.0 if t == 2 else 5.2) for t in team[:40]] + [59 * 0.05] * 200
+        order = sorted(range(len(d)), key=lambda k: -d[k])
+        walls[name] = autotune.simulate_stream(d, team, order, [(3 * n - 2) * b * b * 16 for n, b in shapes], 148)
+    assert walls["short"] < walls["cheap"]
+    assert s["estimate_ms"] <= walls["short"] + 1e-6

@@ -146,6 +146,28 @@ def test_host_streamed_batch_matches_device_batch(precision, wave_bytes):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_host_streamed_batch_with_a_schedule(precision):
+    """One streamed launch with a schedule (sinvb_rgf_batched_stream_sched_*):
+    teams larger than the rule's and a queue order that is not b^3 n; the
+    host copies in the schedule's order (BatchPlan.queue_order) and the
+    results match the device batch."""
+    import torch
+    from sinv_b200.algorithms import rgf_batched_host
+    shapes = [(3, 256), (5, 64), (2, 130), (4, 32), (3, 300), (6, 16), (2, 64)]
+    inst = [workloads.tight_binding(n, b, 0.2 + 0.05 * k, seed=650 + k) for k, (n, b) in enumerate(shapes)]
+    host = [tuple(torch.from_numpy(x.copy()).pin_memory() for x in t) for t in inst]
+    sched = {"team": [4, 1, 2, 1, 4, 1, 1], "priority": [float(k) for k in range(len(shapes))]}
+    plan = BatchPlan([tuple(torch.from_numpy(x).cuda() for x in t) for t in inst], schedule=sched)
+    assert plan.queue_order() == list(range(len(shapes)))[::-1]
+    ref = rgf_batched(inst, precision=precision)
+    out = rgf_batched_host(host, outputs=host, precision=precision, schedule=sched)
+    for G, R in zip(out, ref):
+        for g, r in zip(G, R):
+            if r.size:
+                assert _rel(g.numpy(), r) <= 1e-12, _rel(g.numpy(), r)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_batch_rerun_captured_in_cuda_graph(precision):
     """BatchPlan.capture(): the re-run (memsets + persistent cooperative launch)
     as a CUDA graph; replays reproduce the eager results bit for bit and follow
