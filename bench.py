@@ -662,6 +662,18 @@ def e2e_streamed(torch, spec, args, dev, world):
             for dst, src in zip(h, workloads.tight_binding_device(n, b, e, s, device=dev)):
                 dst.copy_(src)
 
+    sched, sched_note = None, ""
+    if args.tune:  # teams and queue order for a streamed batch (the table is cached by now)
+        from sinv_b200 import autotune
+        shapes = [(spec[k][1], spec[k][2]) for k in idx]
+        table = autotune.load_or_measure(sorted({b for _, b in shapes}), args.precision, args.digits, dev)
+        sched = autotune.stream_schedule(shapes, table, torch.cuda.get_device_properties(dev).multi_processor_count,
+                                         args.precision)
+        by_b = {}
+        for (_, b), t in zip(shapes, sched["team"]):
+            by_b.setdefault(b, set()).add(int(t))
+        sched_note = (", teams and queue order from autotune.stream_schedule (%s; teams by b %s; simulated %.0f ms)"
+                      % (sched["candidate"], {b: sorted(v) for b, v in sorted(by_b.items())}, sched["estimate_ms"]))
     times = []
     for step in range(args.warmup + args.steps):
         regen()
@@ -671,7 +683,7 @@ def e2e_streamed(torch, spec, args, dev, world):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         rgf_batched_host(host, outputs=host, precision=args.precision, digits=args.digits, device=dev,
-                         schedule="tune" if args.tune else None)
+                         schedule=sched)
         t = time.perf_counter() - t0
         if world > 1:
             tt = torch.tensor([t], dtype=torch.float64, device=dev)
@@ -690,8 +702,7 @@ def e2e_streamed(torch, spec, args, dev, world):
                        "every %dth instance (%d)" % (len(spec) // len(idx), len(idx)))
                       + ", %.0f GB each way through pinned host memory; rgf_batched_host (%s%s) overlaps the "
                         "copies with the sweeps; wall clock around the call"
-                      % (bytes_step / 1e9, mode, ", teams and queue order from autotune.stream_schedule"
-                         if args.tune else "")}
+                      % (bytes_step / 1e9, mode, sched_note)}
 
 
 def e2e_sample(torch, spec, args, dev, world):

@@ -344,9 +344,12 @@ def stream_schedule(shapes, table, sms, precision="mixed", elem_bytes=16, h2d_gb
     choices = [sorted(t for t in (int(x) for x in table[_nearest(table, b)]) if t <= sms) for _, b in shapes]
     fastest = [min(ts, key=lambda t: costs(b, t)["row_ms"]) for ts, (_, b) in zip(choices, shapes)]
     bmax = max(b for _, b in shapes)
-    cands = {"tuned " + base["candidate"]: base["team"], "fixed rule": fixed_rule_teams(shapes, sms),
-             "fastest": fastest,
-             "fastest for b=%d" % bmax: [f if b == bmax else t for f, t, (_, b) in zip(fastest, base["team"], shapes)]}
+    bases = {"tuned " + base["candidate"]: base["team"], "fixed rule": fixed_rule_teams(shapes, sms)}
+    cands = dict(bases)
+    cands["fastest"] = fastest
+    for name, team in bases.items():
+        cands[name + ", fastest for b=%d" % bmax] = [f if b == bmax else t
+                                                     for f, t, (_, b) in zip(fastest, team, shapes)]
     best = None
     for name, team in cands.items():
         d = [r * costs(b, t)["row_ms"] for r, (_, b), t in zip(rows, shapes, team)]
