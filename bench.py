@@ -35,6 +35,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -126,8 +127,8 @@ class Clocks:
     def __init__(self, device_index):
         self.idx = device_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "bench_clocks.csv") if os.path.isdir(
-            os.path.join(ROOT, "gpurun_out")) else "/tmp/sinvb_bench_clocks.csv"
+        # the raw samples of the last timed region (the line carries their summary)
+        self.path = os.environ.get("SINVB_BENCH_CLOCKS", os.path.join(tempfile.gettempdir(), "sinvb_bench_clocks.csv"))
 
     def start(self):
         try:
