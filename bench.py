@@ -276,12 +276,13 @@ def cpu_baseline(spec, reps=3, per_b=PER_B):
 # cores (the library's cut-over; smaller blocks keep FP64 DMMA products).
 MIXED_MIN_B = 256
 INT8_PEAK_TOPS = 4500.0  # nominal dense int8 rate of a B200 (no measured figure on this pool)
-# DRAM bytes (read + write) per canonical flop of the batched kernel, from one
-# ncu capture of 37 instances of n = 8, b = 512 (one launch per precision):
-# 132.0 GB and 101.9 GB per launch for 2.54e12 canonical flops.  The operand
+# DRAM bytes (read + write) per canonical flop of the batched kernel, from ncu
+# captures of n = 8, b = 512 batches: mixed, 74 instances on two-CTA teams
+# (the autotuned schedule), 320.7 GB per launch for 5.09e12 canonical flops;
+# FP64, 37 instances on four-CTA teams, 101.9 GB for 2.54e12.  The operand
 # re-reads per output tile grow like b^3, as the flops do, so the launch's
 # traffic is estimated as this ratio times its canonical flops.
-TRAFFIC_BYTES_PER_FLOP = {"mixed": 132.0e9 / 2.54e12, "fp64": 101.9e9 / 2.54e12}
+TRAFFIC_BYTES_PER_FLOP = {"mixed": 320.7e9 / 5.085e12, "fp64": 101.9e9 / 2.54e12}
 
 
 def tensor_work(spec, precision, digits, mixed_min_b=None):
@@ -487,8 +488,9 @@ def run_sinvb(args, rank, world, local_rank):
            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                         "frac": achieved / peak,
                         "traffic": TRAFFIC_BYTES_PER_FLOP[args.precision] * sum(flops) / len(flops),
-                        "traffic_source": "ncu dram__bytes read+write of a 37-instance n=8 b=512 launch, "
-                                          "scaled to this launch by canonical flops",
+                        "traffic_source": "ncu dram__bytes read+write of an n=8 b=512 launch (mixed: 74 "
+                                          "instances on two-CTA teams; FP64: 37 on four-CTA teams), scaled to "
+                                          "this launch by canonical flops",
                         "algorithmic_bytes": sum(workloads.rgf_bytes(n, b) for (_, n, b, _) in spec) / len(flops),
                         "kernel": "rgf_batched_kernel", "flops": "canonical 8 b^3 (8(n-1)+n) per instance",
                         "frac_meaning": "FP64-equivalent: canonical flops per second over the FP64 DMMA peak; "
