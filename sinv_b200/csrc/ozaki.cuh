@@ -49,6 +49,7 @@ constexpr int kOzStageB = kOzTileN * kOzKBlock;       // 2048 B: one digit of a 
 constexpr int kOzEpiCols = 32;                        // output columns per epilogue staging pass
 constexpr int kOzEpiStride = 2 * kOzEpiCols + 1;      // doubles per staged row (odd: no bank conflicts)
 constexpr size_t kOzEpiBytes = (size_t)kOzTileM * kOzEpiStride * 8;
+static_assert(kOzTileN % kOzEpiCols == 0 && (kOzTileM * kOzEpiCols) % 128 == 0, "epilogue passes");
 
 __host__ __device__ inline int oz_pad(int x, int m) { return (x + m - 1) / m * m; }
 
@@ -74,7 +75,8 @@ __host__ __device__ inline OzShape oz_shape(int M, int N, int K, int S) {
   return s;
 }
 
-// Stages of the ring: four, three for 8 digits (shared memory).
+// Stages of the ring: four, three for 8 digits (shared memory).  A fifth stage
+// for 7 digits (with 8-column epilogue passes to make room) measured no faster.
 __host__ __device__ constexpr int oz_stages(int S) { return S <= 7 ? 4 : 3; }
 __host__ __device__ constexpr size_t oz_stage_bytes(int S) { return (size_t)S * (kOzStageA + kOzStageB); }
 // ring, epilogue staging, 128 exponents of the tile being written (the
@@ -524,7 +526,7 @@ __device__ inline bool oz_tiles(const OzOp* ops, int nops, int first, int stride
       if (!ok) break;
       tc_fence_after();
       // Horner over the levels, least significant first: acc = sum_L v_L 2^(-7(L-2))
-      double acc[2 * kOzEpiCols];
+      double acc[kOzTileN];  // the tile's 64 columns, Re or Im part (by `part`)
       {
         int v[32];
 #pragma unroll
@@ -549,13 +551,13 @@ __device__ inline bool oz_tiles(const OzOp* ops, int nops, int first, int stride
       const int ei = exps[64 + i] - 12;
       const bool addend = op.D != nullptr && op.beta != 0.0;
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
+      for (int h = 0; h < kOzTileN / kOzEpiCols; h++) {
 #pragma unroll
         for (int c = 0; c < kOzEpiCols; c++)
           stg[i * kOzEpiStride + 2 * c + part] =
               op.alpha * acc[h * kOzEpiCols + c] * oz_pow2(ei + exps[h * kOzEpiCols + c]);
         oz_epi_sync();
-        // 16 entries per thread: all addend loads first, then the stores
+        // kPer entries per thread: all addend loads first, then the stores
         constexpr int kPer = kOzTileM * kOzEpiCols / 128;
         cplx dv[kPer];
 #pragma unroll
