@@ -22,7 +22,9 @@ dL/dH over 128 energies through the adjoint, forward and backward timed
 apart), large_mixed (n=256, b=1024 instances in
 one in-place wave, mixed vs FP64 and the error on a 4-block sub-instance) and
 bcr_batch (256 small matrices through the batched BCR, beside one BCR call
-per matrix and the batched FP64 RGF).
+per matrix and the batched FP64 RGF).  At one GPU the default energy-batch
+line also carries the plain_large and gradient_set results under
+"other_workloads" (--no-legs leaves them out).
 
 Metric: matrices/s of the whole batch (all ranks).  Under torchrun every rank
 processes its own 512-instance batch (different Hamiltonian seeds): weak
@@ -66,6 +68,8 @@ def parse():
     ap.add_argument("--cpu-per-b", type=int, default=PER_B,
                     help="CPU sample: the first this many instances of each block size")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="energy batch only: skip the single-matrix and gradient workloads appended to its line")
     ap.add_argument("--only", default=None, choices=["rgf", "bcr", "rgf2s", "psr", "pdiv"],
                     help="plain_large: time only this algorithm (a short run for a profiler)")
     ap.add_argument("--tune", dest="tune", action="store_true", default=True,
@@ -1276,6 +1280,28 @@ def reference_other(args, world):
     return base
 
 
+def other_workloads(args, rank, world, local_rank):
+    """The single-matrix workload (one n=64, b=256 matrix: rgf, bcr, two-sided
+    RGF, PSR, PDIV, errors against the oracle, e2e, CPU baseline) and the
+    gradient workload (128 energies, n=32, b=128: loss and dL/dH through the
+    batched adjoint) measured after the energy batch in the same process, each
+    with its own warm-up, CUDA-event timing and clock samples, so that one
+    default run records them all.  A leg that fails is reported by its error;
+    the energy-batch figures stand."""
+    import copy
+    import torch
+    legs = {}
+    for name, fn, count in (("plain_large", run_plain_large, 1), ("gradient_set", run_gradient_set, 128)):
+        torch.cuda.empty_cache()
+        a = copy.copy(args)
+        a.workload, a.count, a.steps, a.warmup, a.only = name, count, 5, 3, None
+        try:
+            legs[name] = fn(a, rank, world, local_rank)
+        except Exception as err:  # noqa: BLE001 -- the headline line still prints
+            legs[name] = {"error": "%s: %s" % (type(err).__name__, str(err)[:300])}
+    return legs
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -1300,6 +1326,8 @@ def main():
         fn = {"energy_batch": run_sinvb, "plain_large": run_plain_large, "gradient_set": run_gradient_set,
               "large_mixed": run_large_mixed, "bcr_batch": run_bcr_batch}[args.workload]
         out = fn(args, rank, world, local_rank)
+        if args.workload == "energy_batch" and world == 1 and not args.shape and not args.no_legs:
+            out["other_workloads"] = other_workloads(args, rank, world, local_rank)
         if rank == 0:
             print(json.dumps(out), flush=True)
     finally:
