@@ -23,7 +23,7 @@ apart), large_mixed (n=256, b=1024 instances in
 one in-place wave, mixed vs FP64 and the error on a 4-block sub-instance) and
 bcr_batch (256 small matrices through the batched BCR, beside one BCR call
 per matrix and the batched FP64 RGF).  At one GPU the default energy-batch
-line also carries the plain_large and gradient_set results under
+line also carries the plain_large, gradient_set and lesser_batch results under
 "other_workloads" (--no-legs leaves them out).
 
 Metric: matrices/s of the whole batch (all ranks).  Under torchrun every rank
@@ -57,7 +57,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="sinvb", choices=["sinvb", "reference"])
     ap.add_argument("--workload", default="energy_batch",
-                    choices=["energy_batch", "plain_large", "gradient_set", "large_mixed", "bcr_batch"])
+                    choices=["energy_batch", "plain_large", "gradient_set", "large_mixed", "bcr_batch",
+                             "lesser_batch"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--digits", type=int, default=7, help="int8 slices per value of the mixed products")
     ap.add_argument("--count", type=int, default=0, help="instances (0: the workload's default)")
@@ -1109,6 +1110,69 @@ def run_gradient_set(args, rank, world, local_rank):
             "clocks": clk}
 
 
+def run_lesser_batch(args, rank, world, local_rank):
+    """Retarded and lesser Green's functions over 128 energies of one shared
+    tight-binding H (n=32, b=128), Sigma< = i f Gamma with Gamma the eta
+    broadening plus the contacts: one batched call (one persistent launch)
+    against one rgf_lesser call per energy, both through the public Python
+    calls with inputs resident on the device.  Every rank runs its own batch
+    (replicas)."""
+    import torch
+    from sinv_b200 import workloads
+    from sinv_b200.algorithms import rgf_lesser, rgf_lesser_batched
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    energies, n, b, hseed = workloads.gradient_set_spec(count=args.count)
+    H = workloads.hamiltonian(n, b, hseed)
+    host = [workloads.tight_binding(n, b, e, H=H) for e in energies]
+    u = torch.from_numpy(host[0][1]).to(dev)
+    l = torch.from_numpy(host[0][2]).to(dev)
+    inst = [(torch.from_numpy(d).to(dev), u, l) for d, _, _ in host]
+    eye = np.eye(b)
+    gamma = np.stack([2 * workloads.ETA * eye + (2 * workloads.SIGMA_EDGE * eye if i in (0, n - 1) else 0)
+                      for i in range(n)])
+    sig = torch.from_numpy((1j * 0.4 * gamma).astype(np.complex128)).to(dev)
+    sigs = [sig] * len(inst)
+    stream = torch.cuda.current_stream()
+    clocks = Clocks(local_rank) if rank == 0 else None
+    tb, ts = [], []
+    for step in range(args.warmup + args.steps):
+        if step == args.warmup and clocks:
+            clocks.start()
+        torch.cuda.synchronize()
+        mb = _events_ms(torch, lambda: rgf_lesser_batched(inst, sigs), stream)
+        ms = _events_ms(torch, lambda: [rgf_lesser(d, uu, ll, sig) for d, uu, ll in inst], stream)
+        if step >= args.warmup:
+            tb.append(_max_over_ranks(torch, world, dev, mb))
+            ts.append(_max_over_ranks(torch, world, dev, ms))
+    clk = clocks.stop() if clocks else None
+    got = rgf_lesser_batched(inst, sigs)
+    err = 0.0
+    for k in range(0, len(inst), 32):
+        one = rgf_lesser(*inst[k], sig)
+        err = max(err, max(float(torch.linalg.norm(g - r) / torch.linalg.norm(r)) for g, r in zip(got[k], one)))
+    mb, ms = statistics.median(tb), statistics.median(ts)
+    count = len(inst)
+    # the sweep pair's work: 16 complex b x b products per block row and one
+    # block inversion (8 b^3 flops each, as the canonical RGF count)
+    F = 17 * 8.0 * b ** 3 * n * count
+    peak = dmma_peak_tflops(torch)
+    return {"metric": "lesser Green's function evaluations/s (G and G< per energy)",
+            "value": world * count / (mb * 1e-3), "unit": "energies/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mb, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": "lesser_batch(%d energies, n=%d, b=%d, shared H)" % (count, n, b),
+                       "parallelism": "replicas%d" % world},
+            "gpu_launches": args.steps, "path": "rgf_lesser_batched: one persistent launch",
+            "one_call_per_energy": {"ms": ms, "energies_per_s": world * count / (ms * 1e-3),
+                                    "batched_speedup": ms / mb},
+            "rel_err_vs_single_call": err, "clocks": clk,
+            "roofline": {"bound": "tensor", "achieved": F / (mb * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                         "frac": F / (mb * 1e-3) / 1e12 / peak, "traffic": None, "kernel": "lesser_batched_kernel",
+                         "flops": "17 complex b^3 products (8 b^3 flops each) per block row and energy",
+                         "peak_source": "sinvb_fp64_mma_peak (DMMA)"}}
+
+
 def run_large_mixed(args, rank, world, local_rank):
     """Instances n=256, b=1024 (12.85 GB of input each), tight-binding generator,
     mixed precision: 64 instances streamed through HBM in waves (equal waves of
@@ -1276,6 +1340,9 @@ def reference_other(args, world):
                                                 "numpy), scaled to the batch's mean size by canonical flops"},
                      "e2e": {"value": v, "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
         return base
+    if args.workload == "lesser_batch":
+        base.update({"unavailable": "the reference computes no lesser Green's function (only rgf's retarded blocks)"})
+        return base
     base.update({"unavailable": "the reference computes no derivatives (no adjoint of rgf exists in it)"})
     return base
 
@@ -1284,14 +1351,16 @@ def other_workloads(args, rank, world, local_rank):
     """The single-matrix workload (one n=64, b=256 matrix: rgf, bcr, two-sided
     RGF, PSR, PDIV, errors against the oracle, e2e, CPU baseline) and the
     gradient workload (128 energies, n=32, b=128: loss and dL/dH through the
-    batched adjoint) measured after the energy batch in the same process, each
+    batched adjoint) and the lesser workload (the same energies' G and G< in
+    one batched call) measured after the energy batch in the same process, each
     with its own warm-up, CUDA-event timing and clock samples, so that one
     default run records them all.  A leg that fails is reported by its error;
     the energy-batch figures stand."""
     import copy
     import torch
     legs = {}
-    for name, fn, count in (("plain_large", run_plain_large, 1), ("gradient_set", run_gradient_set, 128)):
+    for name, fn, count in (("plain_large", run_plain_large, 1), ("gradient_set", run_gradient_set, 128),
+                            ("lesser_batch", run_lesser_batch, 128)):
         torch.cuda.empty_cache()
         a = copy.copy(args)
         a.workload, a.count, a.steps, a.warmup, a.only = name, count, 5, 3, None
@@ -1309,7 +1378,7 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if not args.count:
         args.count = {"energy_batch": 512, "gradient_set": 128, "large_mixed": 64, "plain_large": 1,
-                      "bcr_batch": 256}[args.workload]
+                      "bcr_batch": 256, "lesser_batch": 128}[args.workload]
     if args.impl == "reference":
         if args.workload == "energy_batch":
             run_reference(args, rank, world)
@@ -1324,7 +1393,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
         fn = {"energy_batch": run_sinvb, "plain_large": run_plain_large, "gradient_set": run_gradient_set,
-              "large_mixed": run_large_mixed, "bcr_batch": run_bcr_batch}[args.workload]
+              "large_mixed": run_large_mixed, "bcr_batch": run_bcr_batch,
+              "lesser_batch": run_lesser_batch}[args.workload]
         out = fn(args, rank, world, local_rank)
         if args.workload == "energy_batch" and world == 1 and not args.shape and not args.no_legs:
             out["other_workloads"] = other_workloads(args, rank, world, local_rank)

@@ -132,6 +132,35 @@ int sinvb_rgf_lesser_z(const void* diag, const void* upper, const void* lower, c
                        int b, unsigned flags, void* G_diag, void* G_upper, void* G_lower, void* GL_diag,
                        void* GL_upper, void* workspace, size_t workspace_bytes, sinvb_stream_t stream);
 
+/*
+ * Many energies of a transport calculation's loop at once: for every
+ * descriptor, the outputs of sinvb_rgf_lesser_z on its own matrix and
+ * self-energy (own n and b), all in one persistent launch whose teams of
+ * CTAs take whole instances from a device queue (largest b^3 n first).  No
+ * reference counterpart: the caller-side loop of rgf
+ * (src/sinv/algorithms/rgf/rgf.py:17-64) followed by G Sigma< G^H per energy.
+ * complex128; flags: 0 or SINVB_FORCE_CTA (one-CTA teams).  ``status`` (count
+ * ints on the device, or NULL) receives each instance's SINVB_OK /
+ * SINVB_STATUS_*; the workspace status word holds the first failure.  Outputs
+ * must not overlap the inputs.
+ */
+typedef struct sinvb_lesser_desc {
+  const void* diag;
+  const void* upper;
+  const void* lower;
+  const void* sigma_lesser;  /* n blocks */
+  void* G_diag;
+  void* G_upper;
+  void* G_lower;
+  void* GL_diag;             /* n blocks G<_ii */
+  void* GL_upper;            /* n-1 blocks G<_{i,i+1} */
+  int n;
+  int b;
+} sinvb_lesser_desc;
+size_t sinvb_rgf_lesser_batched_workspace_size(const sinvb_lesser_desc* descs, int count, unsigned flags);
+int sinvb_rgf_lesser_batched_z(const sinvb_lesser_desc* descs, int count, unsigned flags, void* workspace,
+                               size_t workspace_bytes, int* status, sinvb_stream_t stream);
+
 /* ---- adjoint (reverse mode) of the RGF sweeps ------------------------------------ */
 /*
  * No reference counterpart (the reference has no gradients); the adjoint of

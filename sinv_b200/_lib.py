@@ -51,6 +51,8 @@ SIGNATURES = {
     "sinvb_rgf2s_d": (_i, [_vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _sz, _vp]),
     "sinvb_rgf_lesser_workspace_size": (_sz, [_i, _i]),
     "sinvb_rgf_lesser_z": (_i, [_vp, _vp, _vp, _vp, _i, _i, _u, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "sinvb_rgf_lesser_batched_workspace_size": (_sz, [_vp, _i, _u]),
+    "sinvb_rgf_lesser_batched_z": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp]),
     "sinvb_rgf_batched_z": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp]),
     "sinvb_rgf_batched_d": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp]),
     "sinvb_rgf_batched_stream_z": (_i, [_vp, _i, _u, _vp, _sz, _vp, _vp, _vp, _u, _vp]),
@@ -115,6 +117,12 @@ class AdjointDesc(ctypes.Structure):
     _fields_ = [(name, _vp) for name in ("diag", "upper", "lower", "G_diag", "G_upper", "G_lower", "bG_diag",
                                          "bG_upper", "bG_lower", "checkpoints", "aD", "aU", "aL")] + \
         [("n", _i), ("b", _i)]
+
+
+class LesserDesc(ctypes.Structure):
+    """``sinvb_lesser_desc`` of include/sinvb.h."""
+    _fields_ = [(name, _vp) for name in ("diag", "upper", "lower", "sigma_lesser", "G_diag", "G_upper", "G_lower",
+                                         "GL_diag", "GL_upper")] + [("n", _i), ("b", _i)]
 
 
 class BatchSchedule(ctypes.Structure):

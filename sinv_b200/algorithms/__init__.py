@@ -24,4 +24,4 @@ from .batched import BatchPlan, rgf_batched, rgf_batched_host  # noqa: F401
 from . import adjoint  # noqa: F401
 from .adjoint import RGFBatchFunction, RGFFunction, rgf_autograd, rgf_batched_autograd  # noqa: F401
 from . import lesser  # noqa: F401
-from .lesser import rgf_greater, rgf_lesser  # noqa: F401
+from .lesser import rgf_greater, rgf_greater_batched, rgf_lesser, rgf_lesser_batched  # noqa: F401

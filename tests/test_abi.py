@@ -129,3 +129,42 @@ def test_psr_and_bcr_batched_host_checks(lib):
     assert lib.sinvb_bcr_batched_z(cd, -1, 0, aligned, 4096, null, null) == _lib.EINVAL
     assert lib.sinvb_bcr_batched_z(cd, 1, 0, p if ctypes.addressof(buf) % 256 else None, 4096, null,
                                    null) in (_lib.EINVAL, _lib.EWORKSPACE)
+
+
+def test_lesser_batched_host_checks(lib):
+    """Argument checks of sinvb_rgf_lesser_batched_z run before any device
+    call: distinct 16-byte aligned host ranges stand in for the blocks."""
+    big = (ctypes.c_char * (1 << 16))()
+    base = (ctypes.addressof(big) + 255) & ~255
+    ws = ctypes.c_void_p(base)
+    n, b = 3, 4
+    blk = b * b * 16
+    sizes = [n, n - 1, n - 1, n, n, n - 1, n - 1, n, n - 1]   # diag, upper, lower, sigma, G*, GL*
+    offs, o = [], 4096
+    for m in sizes:
+        offs.append(base + o)
+        o += m * blk
+    names = ["diag", "upper", "lower", "sigma_lesser", "G_diag", "G_upper", "G_lower", "GL_diag", "GL_upper"]
+
+    def desc(**change):
+        f = dict(zip(names, offs))
+        f.update(change)
+        d = (_lib.LesserDesc * 1)()
+        d[0] = _lib.LesserDesc(*(f[k] for k in names), n, b)
+        return ctypes.cast(d, ctypes.c_void_p), d
+
+    good, keep = desc()
+    assert lib.sinvb_rgf_lesser_batched_z(good, 0, 0, ws, 4096, None, None) == _lib.EINVAL
+    assert lib.sinvb_rgf_lesser_batched_z(None, 1, 0, ws, 4096, None, None) == _lib.EINVAL
+    assert lib.sinvb_rgf_lesser_batched_z(good, 1, _lib.FORCE_GRID, ws, 4096, None, None) == _lib.EINVAL
+    assert lib.sinvb_rgf_lesser_batched_z(good, 1, 0, ctypes.c_void_p(base + 16), 4096, None,
+                                          None) == _lib.EWORKSPACE
+    for change in ({"sigma_lesser": None}, {"GL_upper": None}, {"diag": offs[0] + 8},
+                   {"G_diag": offs[0]},              # an output over an input
+                   {"GL_upper": offs[5]}):           # two outputs over each other
+        bad, keep2 = desc(**change)
+        assert lib.sinvb_rgf_lesser_batched_z(bad, 1, 0, ws, 4096, None, None) == _lib.EINVAL, change
+    # a valid descriptor: no GPU here (EUNSUPPORTED / ECUDA), or on a GPU a workspace too small
+    assert lib.sinvb_rgf_lesser_batched_z(good, 1, 0, ws, 256, None, None) in (
+        _lib.EUNSUPPORTED, _lib.ECUDA, _lib.EWORKSPACE)
+    assert lib.sinvb_rgf_lesser_batched_workspace_size(good, 0, 0) == 0

@@ -40,6 +40,7 @@ def test_reference_arm_line(workload):
                            "d2h_bytes_per_step": 0}
 
 
-def test_reference_arm_without_counterpart():
-    line = _run("gradient_set")
+@pytest.mark.parametrize("workload", ["gradient_set", "lesser_batch"])
+def test_reference_arm_without_counterpart(workload):
+    line = _run(workload)
     assert line["impl"] == "reference" and "unavailable" in line
