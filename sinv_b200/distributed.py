@@ -64,6 +64,31 @@ def rgf_batched_sharded(instances, group=None, **kw):
     return dict(zip(mine, out))
 
 
+def rgf_lesser_batched_sharded(instances, sigmas, group=None, gather=False, compute=None, **kw):
+    """Retarded and lesser blocks of this rank's share of the energies: all
+    ranks pass the same lists, shares are balanced by cost (largest first) and
+    nothing is exchanged during the sweeps.  Returns ``{index: (G_diag,
+    G_upper, G_lower, GL_diag, GL_upper, GL_lower)}`` for this rank's
+    instances; with ``gather`` every instance's result as host arrays on every
+    rank (one ``all_gather_object``).  ``compute`` is the batched call
+    (default ``rgf_lesser_batched``; keyword arguments pass through)."""
+    if compute is None:
+        from .algorithms.lesser import rgf_lesser_batched as compute
+    rank, world = rank_and_world(group)
+    costs = [instance_cost(np.shape(d)[0], np.shape(d)[1]) for d, _, _ in instances]
+    mine = shard_by_cost(costs, world, rank)
+    out = dict(zip(mine, compute([instances[k] for k in mine], [sigmas[k] for k in mine], **kw))) if mine else {}
+    if not gather or world == 1:
+        return out
+    host = {k: tuple(np.asarray(x.cpu() if hasattr(x, "cpu") else x) for x in v) for k, v in out.items()}
+    parts = [None] * world
+    _dist().all_gather_object(parts, host, group=group)
+    allres = {}
+    for p in parts:
+        allres.update(p)
+    return allres
+
+
 def energy_loss_and_grad(H_onsite, H_coupling, energies, eta=1e-3, sigma=0.1, group=None, compute=None):
     """Sum over energies of L(E) = -Im Tr sum_i G_ii(E) / pi and its gradient
     with respect to the Hamiltonian blocks, sharded over ranks.

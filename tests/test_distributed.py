@@ -119,3 +119,72 @@ def test_single_process_fallback_sums_locally():
                                                      compute=_term_fn(H_on, H_cp))
     ref = sum(dense_term(H_on, H_cp, E)[0] for E in ENERGIES)
     assert abs(loss.item() - ref) <= 1e-12 * abs(ref)
+
+
+def _dense_lesser_all(inst, sigs):
+    """The six block families of G and G< = G Sigma< G^H per instance (dense, test code)."""
+    res = []
+    for (d, u, l), s in zip(inst, sigs):
+        n, b = d.shape[0], d.shape[1]
+        A = np.zeros((n * b, n * b), complex)
+        S = np.zeros_like(A)
+        for i in range(n):
+            A[i * b:(i + 1) * b, i * b:(i + 1) * b] = d[i]
+            S[i * b:(i + 1) * b, i * b:(i + 1) * b] = s[i]
+            if i < n - 1:
+                A[i * b:(i + 1) * b, (i + 1) * b:(i + 2) * b] = u[i]
+                A[(i + 1) * b:(i + 2) * b, i * b:(i + 1) * b] = l[i]
+        G = np.linalg.inv(A)
+        GL = G @ S @ G.conj().T
+        blk = lambda M, i, j: M[i * b:(i + 1) * b, j * b:(j + 1) * b]
+        fam = lambda M: (np.array([blk(M, i, i) for i in range(n)]),
+                         np.array([blk(M, i, i + 1) for i in range(n - 1)]),
+                         np.array([blk(M, i + 1, i) for i in range(n - 1)]))
+        res.append(fam(G) + fam(GL))
+    return res
+
+
+def _lesser_problem():
+    shapes = [(3, 4), (5, 3), (2, 6), (4, 4), (3, 5), (6, 2), (2, 3)]
+    inst = [workloads.tight_binding(n, b, -1.0 + 0.3 * k, seed=60 + k) for k, (n, b) in enumerate(shapes)]
+    sigs = []
+    for (n, b) in shapes:
+        s = np.zeros((n, b, b), complex)
+        s[0] = s[-1] = 0.2j * np.eye(b)
+        sigs.append(s)
+    return inst, sigs
+
+
+def _lesser_rank_main(rank, world, port, out_dir):
+    import pickle
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        inst, sigs = _lesser_problem()
+        mine = distributed.rgf_lesser_batched_sharded(inst, sigs, compute=_dense_lesser_all)
+        every = distributed.rgf_lesser_batched_sharded(inst, sigs, gather=True, compute=_dense_lesser_all)
+        with open(os.path.join(out_dir, "lesser%d.pkl" % rank), "wb") as f:
+            pickle.dump((sorted(mine), every), f)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_lesser_energies_sharded_over_two_gloo_ranks(tmp_path):
+    """Each rank computes its cost-balanced share of the energies; the shares
+    cover every instance once, and the gathered results are every instance's
+    on every rank."""
+    import pickle
+    world = 2
+    mp.spawn(_lesser_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    inst, sigs = _lesser_problem()
+    ref = _dense_lesser_all(inst, sigs)
+    got = [pickle.load(open(tmp_path / ("lesser%d.pkl" % r), "rb")) for r in range(world)]
+    shares = [set(m) for m, _ in got]
+    assert shares[0].isdisjoint(shares[1]) and shares[0] | shares[1] == set(range(len(inst)))
+    assert all(shares)
+    for _, every in got:
+        assert sorted(every) == list(range(len(inst)))
+        for k in range(len(inst)):
+            for g, r in zip(every[k], ref[k]):
+                assert np.allclose(g, r, rtol=1e-12, atol=1e-14)

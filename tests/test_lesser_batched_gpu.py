@@ -140,3 +140,18 @@ def test_greater_minus_lesser_is_G_minus_G_dagger_for_every_energy():
         lhs = gre[k][3] - les[k][3]
         rhs = Gd - np.conj(np.transpose(Gd, (0, 2, 1)))
         assert _rel(lhs, rhs) <= 1e-10, (k, _rel(lhs, rhs))
+
+
+def test_sharded_form_on_one_process_runs_the_batched_call():
+    """distributed.rgf_lesser_batched_sharded with no process group: this
+    process's share is every instance, computed by the batched call."""
+    from sinv_b200 import distributed
+    shapes = [(3, 32), (5, 64), (2, 16)]
+    inst = [workloads.tight_binding(n, b, 0.2 * k, seed=1100 + k) for k, (n, b) in enumerate(shapes)]
+    sig = [_sigma(n, b, 1200 + k) for k, (n, b) in enumerate(shapes)]
+    got = distributed.rgf_lesser_batched_sharded(inst, sig)
+    ref = rgf_lesser_batched(inst, sig)
+    assert sorted(got) == [0, 1, 2]
+    for k in range(3):
+        for g, r in zip(got[k], ref[k]):
+            assert _rel(g, r) == 0.0
