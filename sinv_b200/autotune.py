@@ -320,15 +320,18 @@ def simulate_stream(durations, teams, order, in_bytes, sms, h2d_gbs=55.0, d2h_gb
     return out
 
 
-def stream_schedule(shapes, table, sms, precision="mixed", elem_bytes=16, h2d_gbs=55.0, d2h_gbs=55.0):
+def stream_schedule(shapes, table, sms, precision="mixed", elem_bytes=16, h2d_gbs=55.0, d2h_gbs=55.0,
+                    order_moves=1000):
     """Teams and queue order for a host-streamed batch: the candidates of
     ``schedule`` plus every instance on its fastest team (shortest chain) and
     that for the largest block size only, each queued longest first, judged
     by ``simulate_stream`` (copy-in, sweeps and copy-out overlapped).  Copies
     make late finishers expensive: an instance that ends after the last input
     has arrived still has its results to copy out, so shorter chains can win
-    over the device-resident makespan choice.  Returns the ``schedule`` dict
-    with "estimate_ms" the simulated wall time."""
+    over the device-resident makespan choice.  The winner's copy / queue order
+    then comes from ``stream_order`` (``order_moves`` local-search moves; its
+    priorities rank that order).  Returns the ``schedule`` dict with
+    "estimate_ms" the simulated wall time."""
     base = schedule(shapes, table, sms, precision)
     mixed_min_b = base["mixed_min_b"]
 
@@ -358,6 +361,44 @@ def stream_schedule(shapes, table, sms, precision="mixed", elem_bytes=16, h2d_gb
         if best is None or wall < best[0]:
             best = (wall, name, team, d)
     wall, name, team, d = best
+    # the order: longest first makes the first results wait for a long chain
+    # while copy-out idles; search for one that keeps the copy-out busy
+    order, searched = stream_order(d, team, in_bytes, sms, h2d_gbs, d2h_gbs, moves=order_moves)
+    if searched < wall:
+        wall, name = searched, name + ", order searched"
+        prio = [0.0] * len(shapes)
+        for pos, k in enumerate(order):
+            prio[k] = float(len(shapes) - pos)
+    else:
+        prio = d
     out = dict(base)
-    out.update({"team": team, "priority": d, "estimate_ms": wall, "candidate": name, "chain_ms": max(d)})
+    out.update({"team": team, "priority": prio, "estimate_ms": wall, "candidate": name, "chain_ms": max(d)})
     return out
+
+
+def stream_order(durations, teams, in_bytes, sms, h2d_gbs=55.0, d2h_gbs=55.0, moves=1000, seed=0):
+    """Copy-in (= queue) order of a host-streamed batch, by local search on
+    ``simulate_stream``: start from the better of longest chain first and
+    most bytes per chain-ms first, then ``moves`` times move one instance to
+    another position and keep the move unless the simulated wall time grows
+    (fixed seed: the same inputs give the same order).  About 1.5 ms of host
+    time per move for 256 instances.  Returns (order, wall_ms)."""
+    import random
+    count = len(durations)
+    starts = [sorted(range(count), key=lambda k: -durations[k]),
+              sorted(range(count), key=lambda k: -in_bytes[k] / max(durations[k], 1e-9))]
+    walls = [simulate_stream(durations, teams, o, in_bytes, sms, h2d_gbs, d2h_gbs) for o in starts]
+    cur, best = (starts[0], walls[0]) if walls[0] <= walls[1] else (starts[1], walls[1])
+    cur = list(cur)
+    rnd = random.Random(seed)
+    for _ in range(moves if count > 1 else 0):
+        i, j = rnd.randrange(count), rnd.randrange(count)
+        if i == j:
+            continue
+        cur.insert(j, cur.pop(i))
+        v = simulate_stream(durations, teams, cur, in_bytes, sms, h2d_gbs, d2h_gbs)
+        if v <= best:
+            best = v
+        else:
+            cur.insert(i, cur.pop(j))
+    return cur, best

@@ -131,3 +131,32 @@ def test_stream_schedule_prefers_short_chains_when_copies_dominate():
         walls[name] = autotune.simulate_stream(d, team, order, [(3 * n - 2) * b * b * 16 for n, b in shapes], 148)
     assert walls["short"] < walls["cheap"]
     assert s["estimate_ms"] <= walls["short"] + 1e-6
+
+
+def test_stream_order_search_keeps_copy_out_busy():
+    """Longest-first makes the first results wait for a long chain while the
+    copy-out idles; the searched order is never worse, is the same on every
+    call, and the schedule's priorities rank exactly that order."""
+    tab = {"512": {"8": {"int8": {"row_ms": 4.6, "sm_ms": 36.8}, "fp64": {"row_ms": 6.2, "sm_ms": 49.6}}},
+           "256": {"4": {"fp64": {"row_ms": 1.8, "sm_ms": 7.2}}},
+           "64": {"1": {"fp64": {"row_ms": 0.17, "sm_ms": 0.17}}}}
+    import numpy as np
+    rng = np.random.default_rng(5)
+    shapes = [(int(rng.integers(16, 129)), int(rng.choice([64, 256, 512]))) for _ in range(60)]
+    in_bytes = [(3 * n - 2) * b * b * 16 for n, b in shapes]
+    team = [8 if b == 512 else 4 if b == 256 else 1 for _, b in shapes]
+    d = [(n - 1) * (4.6 if b == 512 else 1.8 if b == 256 else 0.17) for n, b in shapes]
+    longest = sorted(range(len(d)), key=lambda k: -d[k])
+    base = autotune.simulate_stream(d, team, longest, in_bytes, 148)
+    o1, w1 = autotune.stream_order(d, team, in_bytes, 148, moves=300)
+    o2, w2 = autotune.stream_order(d, team, in_bytes, 148, moves=300)
+    assert o1 == o2 and w1 == w2 and sorted(o1) == list(range(len(d)))
+    assert w1 <= base and w1 == autotune.simulate_stream(d, team, o1, in_bytes, 148)
+    s = autotune.stream_schedule(shapes, tab, 148, "mixed", order_moves=300)
+    order = sorted(range(len(shapes)), key=lambda k: -s["priority"][k])
+    def row_ms(b, t):   # the nearest measured team, as the autotuner looks it up
+        row = tab[str(b)]
+        c = row[str(t) if str(t) in row else min(row, key=lambda x: abs(int(x) - t))]
+        return c["int8" if (b >= s["mixed_min_b"] and "int8" in c) else "fp64"]["row_ms"]
+    ds = [(n - 1) * row_ms(b, t) for (n, b), t in zip(shapes, s["team"])]
+    assert abs(autotune.simulate_stream(ds, s["team"], order, in_bytes, 148) - s["estimate_ms"]) < 1e-6
