@@ -84,16 +84,25 @@ def rgf_lesser_batched(instances, sigmas, team=None, check=True, stream=None, st
     descs = (_lib.LesserDesc * len(instances))()
     keep, outs = [], []
     device = None
+    moved = {}   # one device copy of a host array that several instances share
+
+    def to_dev(x):
+        if dev.is_torch(x) and x.is_cuda:
+            return dev.to_device(x, torch.complex128)
+        if id(x) not in moved:
+            moved[id(x)] = (x, dev.to_device(x, torch.complex128))
+        return moved[id(x)][1]
+
     for k, ((A_diag, A_upper, A_lower), sig) in enumerate(zip(instances, sigmas)):
         if dev.torch_dtype(A_diag) != torch.complex128:
             raise TypeError("rgf_lesser_batched takes complex128 blocks (instance %d)" % k)
-        d = dev.to_device(A_diag, torch.complex128)
+        d = to_dev(A_diag)
         n, b = int(d.shape[0]), int(d.shape[1])
-        s = dev.to_device(sig, torch.complex128)
+        s = to_dev(sig)
         if tuple(s.shape) != (n, b, b):
             raise ValueError("Sigma_lesser of instance %d must be (%d, %d, %d)" % (k, n, b, b))
-        u = dev.to_device(A_upper, torch.complex128) if n > 1 else None
-        l = dev.to_device(A_lower, torch.complex128) if n > 1 else None
+        u = to_dev(A_upper) if n > 1 else None
+        l = to_dev(A_lower) if n > 1 else None
         out = [torch.empty((m, b, b), dtype=torch.complex128, device=d.device) for m in (n, n - 1, n - 1, n, n - 1)]
         descs[k] = _lib.LesserDesc(*(dev.ptr(t) for t in (d, u, l, s)), *(dev.ptr(t) for t in out), n, b)
         keep.append((d, u, l, s))
@@ -119,7 +128,7 @@ def rgf_lesser_batched(instances, sigmas, team=None, check=True, stream=None, st
     for (Gd, Gu, Gl, GLd, GLu), (A_diag, _, _) in zip(outs, instances):
         GLl = -GLu.conj().transpose(1, 2).contiguous()
         res.append(tuple(dev.to_output(t, A_diag) for t in (Gd, Gu, Gl, GLd, GLu, GLl)))
-    del keep
+    del keep, moved
     return res
 
 

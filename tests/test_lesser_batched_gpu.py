@@ -86,6 +86,12 @@ def test_energies_of_one_hamiltonian_share_their_coupling_blocks():
         one = rgf_lesser(*host[k], sig[k].cpu().numpy())
         for g, r in zip(got[k], one):
             assert _rel(g.cpu().numpy(), r) <= 1e-11, k
+    # numpy inputs sharing one host array per coupling block family (moved to the device once)
+    hu, hl = host[0][1], host[0][2]
+    got_np = rgf_lesser_batched([(d_, hu, hl) for d_, _, _ in host], [x.cpu().numpy() for x in sig])
+    for k in range(len(host)):
+        for g, r in zip(got_np[k], got[k]):
+            assert _rel(g, r.cpu().numpy()) == 0.0, k
 
 
 def test_more_instances_than_scratch_slots():
