@@ -19,12 +19,12 @@
 // independent block operations (executor.cuh) that one cooperative kernel
 // runs on every SM:
 //
-//   reduce l:   Dinv[e] = D[e]^{-1}                                   (:121, :148)
+//   reduce l:   Dinv[e] = D[e]^{-1}, one Newton step X0 + X0 (I - D X0) (:121, :148)
 //               U_{e,e+o} = Dinv[e] A_{e,e+o},  L_{e+o,e} = A_{e+o,e} Dinv[e]
 //               U_{e,e-o} = Dinv[e] A_{e,e-o},  L_{e-o,e} = A_{e-o,e} Dinv[e]  (:124-128, :150-154)
 //               D[j] -= L_{j,i} A_{i,j} + L_{j,k} A_{k,j}             (:130-133, :156-159)
 //               A_{j,j-2o} = -L_{j,i} A_{i,j-2o},  A_{j,j+2o} = -L_{j,k} A_{k,j+2o}   (:138-142, :164-168)
-//   root:       G_rr = D[r]^{-1}                                      (:220-249)
+//   root:       G_rr = D[r]^{-1}, one Newton step                     (:220-249)
 //   produce l:  corner / center production                            (:253-383)
 //
 // Level couplings A_{r,r+o} / A_{r+o,r} (l >= 1) and produced couplings
@@ -42,6 +42,7 @@ namespace {
 struct BcrPlan {
   // data offsets in elements from the data base
   size_t D, Dinv, Ua, Ub, La, Lb, W;
+  size_t X0, Ev, eye;  // Newton step: raw inverses, residuals I - D X0, one identity block
   std::vector<size_t> Up, Lo, CU, CL;  // per level (index 0 unused)
   size_t data_elems;
   int height, root;
@@ -71,6 +72,9 @@ BcrPlan bcr_plan(int n, int b) {
   P.Ub = take(n);
   P.La = take(n);
   P.Lb = take(n);
+  P.X0 = take((size_t)(n / 2 + 2));
+  P.Ev = take((size_t)(n / 2 + 2));
+  P.eye = take(1);
   P.Up.assign(P.height + 2, 0);
   P.Lo.assign(P.height + 2, 0);
   P.CU.assign(P.height + 2, 0);
@@ -86,6 +90,23 @@ BcrPlan bcr_plan(int n, int b) {
   off += (size_t)(n / 2 + 2) * invert_side_elems(b);
   P.data_elems = off;
   return P;
+}
+
+template <class T>
+T bcr_one();
+template <>
+cplx bcr_one<cplx>() { return cplx{1.0, 0.0}; }
+template <>
+double bcr_one<double>() { return 1.0; }
+
+// The identity block of the Newton steps (a copy from pageable memory has
+// read the host array when cudaMemcpyAsync returns).
+template <class T>
+int upload_identity(unsigned char* dst, int b, cudaStream_t stream) {
+  std::vector<T> eye((size_t)b * b, T{});
+  for (int i = 0; i < b; i++) eye[(size_t)i * b + i] = bcr_one<T>();
+  SINVB_CUDA(cudaMemcpyAsync(dst, eye.data(), eye.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+  return SINVB_OK;
 }
 
 template <class T>
@@ -109,6 +130,18 @@ void build_bcr(Sched& s, const BcrPlan& P, int n, int b, const T* diag, const T*
   auto CL = [&](int l, int r) -> T* { return l == 0 ? Gl + (size_t)r * bb : blk(P.CL[l], q(r, l)); };
   std::vector<T*> Wv;
   for (int x = 0; x < n / 2 + 2; x++) Wv.push_back(base + P.W + (size_t)x * invert_side_elems(b));
+  auto X0v = [&](size_t x) { return blk(P.X0, (int)x); };
+  auto Evv = [&](size_t x) { return blk(P.Ev, (int)x); };
+  T* I = base + P.eye;
+  // One Newton step on the inverses X0v(x) of raw[x] (pivot-free Gauss-Jordan
+  // loses digits on the undamped blocks BCR inverts, which the reference's
+  // LAPACK inverse keeps): E = I - D X0, then dst[x] = X0 + X0 E.
+  auto newton = [&](const std::vector<T*>& raw, const std::vector<T*>& dst) {
+    s.begin();
+    for (size_t x = 0; x < raw.size(); x++) s.gemm(b, -1.0, raw[x], X0v(x), I, Evv(x));
+    s.begin();
+    for (size_t x = 0; x < raw.size(); x++) s.gemm(b, 1.0, X0v(x), Evv(x), X0v(x), dst[x]);
+  };
 
   s.begin();
   s.copy(n * b, b, diag, b, D, b);  // working diagonal (the reference reduces a copy, bcr_utils.py:66-69)
@@ -116,14 +149,17 @@ void build_bcr(Sched& s, const BcrPlan& P, int n, int b, const T* diag, const T*
     const int o = 1 << l;
     std::vector<int> E;
     for (int e = o - 1; e < n; e += 2 * o) E.push_back(e);
-    // Dinv[e] = D[e]^{-1}
+    // Dinv[e] = D[e]^{-1}, refined by one Newton step
     s.begin();
-    std::vector<T*> inv;
-    for (int e : E) {
-      s.copy(b, b, Dk(e), b, Dinv(e), b);
-      inv.push_back(Dinv(e));
+    std::vector<T*> inv, raw, dst;
+    for (size_t x = 0; x < E.size(); x++) {
+      s.copy(b, b, Dk(E[x]), b, X0v(x), b);
+      inv.push_back(X0v(x));
+      raw.push_back(Dk(E[x]));
+      dst.push_back(Dinv(E[x]));
     }
     invert_many<T>(s, inv, Wv, b);
+    newton(raw, dst);
     // U / L factors of every eliminated row
     s.begin();
     for (int e : E) {
@@ -150,10 +186,11 @@ void build_bcr(Sched& s, const BcrPlan& P, int n, int b, const T* diag, const T*
       if (r <= n - 1) s.gemm(b, -1.0, La(k), Up(l, k), nullptr, Up(l + 1, j));
     }
   }
-  // root
+  // root, refined by one Newton step
   s.begin();
-  s.copy(b, b, Dk(P.root), b, Gd + (size_t)P.root * bb, b);
-  invert_many<T>(s, std::vector<T*>{Gd + (size_t)P.root * bb}, Wv, b);
+  s.copy(b, b, Dk(P.root), b, X0v(0), b);
+  invert_many<T>(s, std::vector<T*>{X0v(0)}, Wv, b);
+  newton(std::vector<T*>{Dk(P.root)}, std::vector<T*>{Gd + (size_t)P.root * bb});
   // production, top level down
   for (int l = P.height - 1; l >= 0; l--) {
     const int o = 1 << l;
@@ -265,6 +302,8 @@ int run_bcr(const void* diag, const void* upper, const void* lower, int n, int b
                              stream));
   SINVB_CUDA(cudaMemcpyAsync(ws + L.phases_off, s.phases.data(), s.phases.size() * sizeof(ExecPhase),
                              cudaMemcpyHostToDevice, stream));
+  rc = upload_identity<T>(ws + L.data_off + bcr_plan(n, b).eye * sizeof(T), b, stream);
+  if (rc) return rc;
   if (tile_for(b) == 64) return launch_bcr<T, 64, 64>(ws, (int)s.phases.size(), stream);
   return launch_bcr<T, 32, 32>(ws, (int)s.phases.size(), stream);
 }
@@ -386,6 +425,10 @@ int run_bcr_batched(const sinvb_batch_desc* d, int count, void* workspace, size_
   SINVB_CUDA(cudaMemcpyAsync(ws + L.phases_off, s.phases.data(), s.phases.size() * sizeof(ExecPhase),
                              cudaMemcpyHostToDevice, stream));
   SINVB_CUDA(cudaMemsetAsync(ws + L.status_off, 0, (size_t)count * sizeof(int), stream));
+  for (int k = 0; k < count; k++) {
+    rc = upload_identity<T>(ws + L.data_off[k] + bcr_plan(d[k].n, d[k].b).eye * sizeof(T), d[k].b, stream);
+    if (rc) return rc;
+  }
   if (L.tile == 64) return launch_bcr<T, 64, 64>(ws, (int)s.phases.size(), stream);
   return launch_bcr<T, 32, 32>(ws, (int)s.phases.size(), stream);
 }

@@ -54,13 +54,14 @@ def test_many_equal_matrices_tight_binding():
     """BCR inverts the undamped diagonal blocks and their reduced forms; on some
     of these energies the oracle's own BCR lands 2-3e-10 from the dense inverse
     (RGF: 1e-13).  The bar is the reference algorithm's accuracy class: within
-    10x of the oracle BCR's distance to the dense inverse, plus 1e-11."""
+    6x of the oracle BCR's distance to the dense inverse, plus 1e-11 (measured
+    with the Newton step on every block inverse: at most 4.3x, median 1.45x)."""
     inst = [workloads.tight_binding(12, 64, 0.1 + 0.02 * k, seed=k) for k in range(24)]
     out = bcr_batched(inst)
     for (d, u, l), G in zip(inst, out):
         D = dense.inv_selected(d, u, l)
         ref = _worst(bcr_oracle.bcr_blocks(d, u, l)[:3], D)
-        assert _worst(G, D) <= 10 * ref + 1e-11, (_worst(G, D), ref)
+        assert _worst(G, D) <= 6 * ref + 1e-11, (_worst(G, D), ref)
     d, u, l = inst[1]
     assert _worst(out[1], rgf_oracle.rgf(d, u, l)) <= 1e-10
 

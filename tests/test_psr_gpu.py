@@ -82,7 +82,8 @@ def test_tight_binding(n, b, P):
     G = psr_s.psr_blocks(d, u, l, partitions=P)
     D = dense.inv_selected(d, u, l)
     ref = _worst(psr_oracle.psr(d, u, l, psr_s.partitions_for(n, P)), D)
-    assert _worst(G, D) <= 10 * ref + 1e-11, (_worst(G, D), ref)
+    # measured: at most 2.8x the oracle PSR's own distance (one Newton step per block inverse)
+    assert _worst(G, D) <= 4 * ref + 1e-11, (_worst(G, D), ref)
 
 
 def test_torch_inputs_single_precision_and_dense_torch():
