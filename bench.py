@@ -860,12 +860,16 @@ def run_plain_large(args, rank, world, local_rank):
     F = workloads.rgf_flops(n, b)
     # e2e: host (pinned) inputs in, host outputs back, through the public call
     hd, hu, hl = (torch.from_numpy(x).pin_memory() for x in (dn, un, ln))
+    outs = [torch.empty_like(x).pin_memory() for x in (hd, hu, hl)]   # the caller's pinned result buffers
     te = []
     for step in range(args.warmup + args.steps):
         def e2e():
             G = rgf.rgf_blocks(hd.to(dev, non_blocking=True), hu.to(dev, non_blocking=True),
                                hl.to(dev, non_blocking=True), check=False)
-            return [g.to("cpu") for g in G]
+            for o, g in zip(outs, G):
+                o.copy_(g, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            return outs
         m = _events_ms(torch, e2e, stream)
         if step >= args.warmup:
             te.append(m)
