@@ -97,6 +97,8 @@ def rgf_lesser_batched(instances, sigmas, team=None, check=True, stream=None, st
         if dev.torch_dtype(A_diag) != torch.complex128:
             raise TypeError("rgf_lesser_batched takes complex128 blocks (instance %d)" % k)
         d = to_dev(A_diag)
+        if device is not None and d.device != device:
+            raise ValueError("rgf_lesser_batched: every instance must be on one device (instance %d)" % k)
         n, b = int(d.shape[0]), int(d.shape[1])
         s = to_dev(sig)
         if tuple(s.shape) != (n, b, b):
