@@ -1114,6 +1114,11 @@ def run_gradient_set(args, rank, world, local_rank):
             "clocks": clk}
 
 
+# DRAM bytes per energy of the batched lesser kernel at n=32, b=128 (ncu
+# dram__bytes_read.sum + dram__bytes_write.sum of a 32-energy launch: 1.89 + 4.26 GB)
+LESSER_TRAFFIC_PER_ENERGY = 6.145e9 / 32
+
+
 def run_lesser_batch(args, rank, world, local_rank):
     """Retarded and lesser Green's functions over 128 energies of one shared
     tight-binding H (n=32, b=128), Sigma< = i f Gamma with Gamma the eta
@@ -1172,7 +1177,11 @@ def run_lesser_batch(args, rank, world, local_rank):
                                     "batched_speedup": ms / mb},
             "rel_err_vs_single_call": err, "clocks": clk,
             "roofline": {"bound": "tensor", "achieved": F / (mb * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
-                         "frac": F / (mb * 1e-3) / 1e12 / peak, "traffic": None, "kernel": "lesser_batched_kernel",
+                         "frac": F / (mb * 1e-3) / 1e12 / peak,
+                         "traffic": LESSER_TRAFFIC_PER_ENERGY * count * (n * b * b) / (32 * 128 * 128),
+                         "traffic_source": "ncu dram__bytes read+write of a 32-energy n=32 b=128 launch (6.15 GB), "
+                                           "per energy, scaled by n b^2",
+                         "kernel": "lesser_batched_kernel",
                          "flops": "17 complex b^3 products (8 b^3 flops each) per block row and energy",
                          "peak_source": "sinvb_fp64_mma_peak (DMMA)"}}
 
