@@ -324,7 +324,7 @@ def stream_schedule(shapes, table, sms, precision="mixed", elem_bytes=16, h2d_gb
                     order_moves=1000):
     """Teams and queue order for a host-streamed batch: the candidates of
     ``schedule`` plus every instance on its fastest team (shortest chain) and
-    that for the largest block size only, each queued longest first, judged
+    that for the largest block size only, each queued longest first, compared
     by ``simulate_stream`` (copy-in, sweeps and copy-out overlapped).  Copies
     make late finishers expensive: an instance that ends after the last input
     has arrived still has its results to copy out, so shorter chains can win
