@@ -23,7 +23,8 @@ apart), large_mixed (n=256, b=1024 instances in
 one in-place wave, mixed vs FP64 and the error on a 4-block sub-instance) and
 bcr_batch (256 small matrices through the batched BCR, beside one BCR call
 per matrix and the batched FP64 RGF).  At one GPU the default energy-batch
-line also carries the plain_large, gradient_set and lesser_batch results under
+line also carries the plain_large, gradient_set, lesser_batch and one wave of
+the large_mixed results under
 "other_workloads" (--no-legs leaves them out).
 
 Metric: matrices/s of the whole batch (all ranks).  Under torchrun every rank
@@ -1364,19 +1365,23 @@ def other_workloads(args, rank, world, local_rank):
     """The single-matrix workload (one n=64, b=256 matrix: rgf, bcr, two-sided
     RGF, PSR, PDIV, errors against the oracle, e2e, CPU baseline) and the
     gradient workload (128 energies, n=32, b=128: loss and dL/dH through the
-    batched adjoint) and the lesser workload (the same energies' G and G< in
-    one batched call) measured after the energy batch in the same process, each
+    batched adjoint), the lesser workload (the same energies' G and G< in
+    one batched call) and one in-place wave (11 instances) of the large mixed
+    workload (n=256, b=1024) measured after the energy batch in the same process, each
     with its own warm-up, CUDA-event timing and clock samples, so that one
     default run records them all.  A leg that fails is reported by its error;
     the energy-batch figures stand."""
     import copy
     import torch
     legs = {}
-    for name, fn, count in (("plain_large", run_plain_large, 1), ("gradient_set", run_gradient_set, 128),
-                            ("lesser_batch", run_lesser_batch, 128)):
+    # (workload, function, instances, timed steps, warm-up steps); the large
+    # mixed workload runs one in-place wave of its n=256, b=1024 instances
+    legs_spec = (("plain_large", run_plain_large, 1, 5, 3), ("gradient_set", run_gradient_set, 128, 5, 3),
+                 ("lesser_batch", run_lesser_batch, 128, 5, 3), ("large_mixed", run_large_mixed, 11, 1, 1))
+    for name, fn, count, steps, warmup in legs_spec:
         torch.cuda.empty_cache()
         a = copy.copy(args)
-        a.workload, a.count, a.steps, a.warmup, a.only = name, count, 5, 3, None
+        a.workload, a.count, a.steps, a.warmup, a.only = name, count, steps, warmup, None
         try:
             legs[name] = fn(a, rank, world, local_rank)
         except Exception as err:  # noqa: BLE001 -- the headline line still prints
