@@ -320,8 +320,26 @@ def simulate_stream(durations, teams, order, in_bytes, sms, h2d_gbs=55.0, d2h_gb
     return out
 
 
+_stream_memo = {}
+
+
 def stream_schedule(shapes, table, sms, precision="mixed", elem_bytes=16, h2d_gbs=55.0, d2h_gbs=55.0,
                     order_moves=1000):
+    """``_stream_schedule``, remembered for the last few distinct arguments:
+    an energy loop that streams batches of the same shapes on the same table
+    pays for the order search once.  Returns a fresh copy of the schedule."""
+    key = (tuple((int(n), int(b)) for n, b in shapes), json.dumps(table, sort_keys=True), int(sms), precision,
+           int(elem_bytes), float(h2d_gbs), float(d2h_gbs), int(order_moves))
+    if key not in _stream_memo:
+        if len(_stream_memo) >= 8:
+            _stream_memo.pop(next(iter(_stream_memo)))
+        _stream_memo[key] = _stream_schedule(shapes, table, sms, precision, elem_bytes, h2d_gbs, d2h_gbs, order_moves)
+    out = _stream_memo[key]
+    return {k: (list(v) if isinstance(v, list) else v) for k, v in out.items()}
+
+
+def _stream_schedule(shapes, table, sms, precision="mixed", elem_bytes=16, h2d_gbs=55.0, d2h_gbs=55.0,
+                     order_moves=1000):
     """Teams and queue order for a host-streamed batch: the candidates of
     ``schedule`` plus every instance on its fastest team (shortest chain) and
     that for the largest block size only, each queued longest first, compared

@@ -160,3 +160,26 @@ def test_stream_order_search_keeps_copy_out_busy():
         return c["int8" if (b >= s["mixed_min_b"] and "int8" in c) else "fp64"]["row_ms"]
     ds = [(n - 1) * row_ms(b, t) for (n, b), t in zip(shapes, s["team"])]
     assert abs(autotune.simulate_stream(ds, s["team"], order, in_bytes, 148) - s["estimate_ms"]) < 1e-6
+
+
+def test_stream_schedule_is_remembered_for_the_same_batch(monkeypatch):
+    """The same shapes on the same table: the order search runs once, and each
+    call gets its own copy of the schedule."""
+    tab = {"256": {"4": {"fp64": {"row_ms": 1.8, "sm_ms": 7.2}}}, "64": {"1": {"fp64": {"row_ms": 0.17, "sm_ms": 0.17}}}}
+    shapes = [(20 + k, 256 if k % 3 else 64) for k in range(30)]
+    calls = []
+    real = autotune.stream_order
+
+    def counting(*a, **k):
+        calls.append(1)
+        return real(*a, **k)
+
+    monkeypatch.setattr(autotune, "stream_order", counting)
+    autotune._stream_memo.clear()
+    s1 = autotune.stream_schedule(shapes, tab, 148, "fp64", order_moves=50)
+    s2 = autotune.stream_schedule(shapes, tab, 148, "fp64", order_moves=50)
+    assert len(calls) == 1 and s1 == s2 and s1["team"] is not s2["team"]
+    s2["team"][0] = -1
+    assert autotune.stream_schedule(shapes, tab, 148, "fp64", order_moves=50)["team"][0] != -1
+    autotune.stream_schedule(shapes[:-1], tab, 148, "fp64", order_moves=50)
+    assert len(calls) == 2
